@@ -1,0 +1,183 @@
+/*
+ * mmp.h — C ABI of the B200 Lawson–Runge–Kutta multimode NLSE solver.
+ *
+ * Plain C, plain pointers and sizes; no CUDA or C++ types cross this boundary.
+ * The C++ drop-in classes (MultimodePropagation_B200.hpp) and the Python
+ * bindings (mm_propagation_b200/capi.py) are thin layers over these entry
+ * points. Each entry point replaces a piece of alexandreroget/MM_Propagation's
+ * C++ solver API; the replaced interface is cited beside it.
+ *
+ * Conventions
+ *  - Every call returns 0 (MMP_OK) or a negative MMP_E* code; mmp_strerror()
+ *    turns it into text. The reference checks no return codes at all.
+ *  - Complex arrays are interleaved FP64 (re, im) with the mode index
+ *    outermost: field[p][t][2], p < n_modes, t < nt. This is the memory order
+ *    of ComplexArraysContainer ([mode][sample], include/ComplexArraysContainer.hpp:7-29).
+ *  - Callers own every buffer they pass; inputs are copied during the call.
+ *  - A solver (or batch) is not thread-safe; use one per host thread. Each
+ *    owns one CUDA stream on the device that was current when it was created.
+ */
+#ifndef MMP_B200_H
+#define MMP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define MMP_OK 0
+#define MMP_EINVAL (-1)     /* malformed parameters (see mmp_validate_params) */
+#define MMP_ENOMEM (-2)     /* device or host allocation failed */
+#define MMP_ECUDA (-3)      /* a CUDA runtime call failed */
+#define MMP_ENONFINITE (-4) /* the field became NaN/Inf during propagation */
+#define MMP_ETIMEOUT (-5)   /* a bounded wait expired (server, device-side waits) */
+#define MMP_ENOTSUP (-6)    /* valid input outside what this build supports (e.g. NT not 2^k) */
+#define MMP_ENODEV (-7)     /* no usable sm_100 device */
+#define MMP_ESTATE (-8)     /* call not valid in the object's current state */
+
+/* ---- flags (mmp_params.flags) ---------------------------------------------------- */
+/* Arithmetic: default is FP32 bulk (FFTs, contraction, Raman) with FP64 dispersion
+ * phase, FP64 field accumulation and FP64 monitors. MMP_F_FP64 runs everything in FP64. */
+#define MMP_F_FP64 (1u << 0)
+/* Pair table: the reference forms V[slot] from slot%M and slot/M instead of from
+ * unique_pairs[slot] (src/MultimodePropagation_CPU.cpp:126-133, :195-205). That is
+ * the default here, for parity; MMP_F_PHYSICAL_PAIRS uses unique_pairs[slot]. */
+#define MMP_F_PHYSICAL_PAIRS (1u << 1)
+/* z handling: the reference resets z to 0 at every computeLawsonRK call while the
+ * interaction-picture field carries on (src/MultimodePropagation.cpp:158-163).
+ * That is the default; MMP_F_CONTINUOUS carries z across calls instead. */
+#define MMP_F_CONTINUOUS (1u << 2)
+/* Skip the per-step FP64 energy / photon-number monitors. */
+#define MMP_F_NO_MONITORS (1u << 3)
+
+/* RK tableau selection (mmp_params.rk_variant) */
+#define MMP_RK_BY_ORDER 0      /* method_order 8 -> Butcher11, 6 -> Butcher7(nu=1), else RK4
+                                  (src/MultimodePropagation.cpp:15-27) */
+#define MMP_RK_BUTCHER7_LAMBDA_MU 1 /* the two-parameter 7-stage tableau
+                                       (src/RungeKutta.cpp:75-122), params rk_lambda, rk_mu */
+
+/* One non-zero coupling coefficient Q^(p)_{k,l,m}: struct NonZeroValue plus the
+ * output-mode index p (include/Sparse3DArray.hpp:7-11). Entries of the same p
+ * keep the order in which they appear in the array: that order is the
+ * reference's insertion order and decides the pair table. */
+typedef struct mmp_nz {
+  uint32_t p, k, l, m;
+  double value;
+} mmp_nz;
+
+/* struct SimulationParameters (include/MultimodePropagation.hpp:16-33), flattened.
+ * Units as in the reference's README (README.md:73-88). */
+typedef struct mmp_params {
+  uint32_t n_modes;             /* M */
+  uint32_t nt;                  /* NT: samples per mode (power of two, 2^6..2^16) */
+  uint32_t n_beta;              /* L: dispersion orders per mode (>= 3) */
+  const double* dispersion;     /* [M][L] beta_i^(p) in ps^i/m */
+  uint32_t n_nonzeros;
+  const mmp_nz* coupling;       /* [n_nonzeros], Q in 1/m^2 */
+  const double* initial_fields; /* [M][NT][2] in W^(1/2) */
+  double time_window;           /* ps */
+  double pulse_width;           /* T0, ps */
+  double fiber_length;          /* m */
+  uint32_t n_steps;
+  uint32_t method_order;
+  double nonlinearity_const;    /* gamma, 1/(W m) */
+  double raman_proportion;      /* f_R (ignored when raman == 0) */
+  const double* raman_response; /* [NT] h_R on the time grid, 1/ps; NULL when raman == 0 */
+  int32_t raman;                /* 0: MultimodePropagation*_RamanOFF, 1: *_RamanON */
+  uint32_t flags;               /* MMP_F_* */
+  int32_t rk_variant;           /* MMP_RK_* */
+  double rk_lambda, rk_mu;      /* for MMP_RK_BUTCHER7_LAMBDA_MU */
+  double center_frequency;      /* omega0 in rad/ps for the photon-number monitor; 0 = off */
+} mmp_params;
+
+/* Read-only facts about a solver after creation (the base class's protected
+ * members, include/MultimodePropagation.hpp:66-93). */
+typedef struct mmp_info {
+  uint32_t n_modes, nt, n_stages, n_pairs; /* n_pairs = |unique_pairs| */
+  uint32_t n_pair_fields;                  /* distinct (l<=m) pair fields the device forms */
+  uint32_t pair_quirk_active;              /* 1 if some unique_pairs[slot] != slot and the
+                                              reference slot mapping is in use */
+  double t_final, delta_t, z_final, delta_z, z; /* dimensionless, as in the reference */
+  double LD, conversion_factor, max_beta2, max_Q;
+  uint64_t steps_done;                      /* steps since creation (monotone) */
+  uint32_t fp64;                            /* 1 if MMP_F_FP64 */
+  uint32_t cluster_ctas;                    /* CTAs that share one FFT row */
+} mmp_info;
+
+typedef struct mmp_solver mmp_solver;
+
+/* Validate parameters without touching the device. Checks the conditions the
+ * MATLAB front-end checks (matlab/mm_propagation.cpp:341-527) plus the ones
+ * under which the reference silently produces NaN/Inf (max|beta2| == 0,
+ * max|Q| == 0, T0 <= 0, fewer than 3 dispersion orders, indices >= M).
+ * On failure writes a one-line reason into msg (if msg != NULL). */
+int mmp_validate_params(const mmp_params* params, char* msg, size_t msg_len);
+
+/* MultimodePropagationCPU_RamanOFF/ON constructors
+ * (src/MultimodePropagation_CPU.cpp:4-21, :163, :225-232; src/MultimodePropagation.cpp:4-12).
+ * Uploads everything and leaves the solver at z = 0. */
+int mmp_solver_create(const mmp_params* params, mmp_solver** out);
+
+/* virtual void computeLawsonRK(unsigned nz) (include/MultimodePropagation.hpp:41,
+ * src/MultimodePropagation_CPU.cpp:24-34): nz Lawson–RK steps of delta_z.
+ * Resets z to 0 first unless MMP_F_CONTINUOUS. Returns MMP_ENONFINITE if the
+ * field stopped being finite. Blocks until the device is done. */
+int mmp_propagate(mmp_solver* s, uint32_t nz);
+
+/* Asynchronous form of mmp_propagate: enqueues the steps on the solver's stream
+ * and returns; mmp_synchronize waits and reports the status. */
+int mmp_propagate_async(mmp_solver* s, uint32_t nz);
+int mmp_synchronize(mmp_solver* s);
+
+/* void computeLawsonRK() (src/MultimodePropagation.cpp:213-216):
+ * nz = floor(z_final / delta_z). */
+int mmp_propagate_default(mmp_solver* s);
+
+/* virtual ComplexArraysContainer getResult() (src/MultimodePropagation_CPU.cpp:88-104):
+ * phi_p = IFFT(exp(L_p z) * FFT(psi_p)) / conversion_factor, into out[M][NT][2]. */
+int mmp_get_result(mmp_solver* s, double* out);
+
+/* Replace the field with new initial fields phi0[M][NT][2] (W^(1/2)) and set z = 0,
+ * keeping every other parameter: the same as constructing a new solver with
+ * other initial_fields, without re-uploading the rest. */
+int mmp_set_fields(mmp_solver* s, const double* phi0);
+
+/* Per-step FP64 monitors since creation: total energy (pJ, sum over modes of
+ * |phi|^2 dt) and photon number (0 when center_frequency == 0), at the end of
+ * each step. Copies min(max_steps, steps_done) entries; n_written may be NULL. */
+int mmp_get_monitors(mmp_solver* s, double* energy, double* photons, uint64_t max_steps,
+                     uint64_t* n_written);
+
+int mmp_get_info(mmp_solver* s, mmp_info* info);
+
+/* ~MultimodePropagation (include/MultimodePropagation.hpp:39). NULL is allowed. */
+void mmp_solver_destroy(mmp_solver* s);
+
+/* ---- batches: many independent solves advanced by the same launches -------------- */
+/* All members must share nt, flags & MMP_F_FP64, raman and the RK tableau; n_modes,
+ * coupling, dispersion, fields and lengths may differ. Member i is addressed by index. */
+typedef struct mmp_batch mmp_batch;
+int mmp_batch_create(const mmp_params* const* params, uint32_t n, mmp_batch** out);
+int mmp_batch_propagate(mmp_batch* b, uint32_t nz);
+int mmp_batch_propagate_async(mmp_batch* b, uint32_t nz);
+int mmp_batch_synchronize(mmp_batch* b);
+int mmp_batch_get_result(mmp_batch* b, uint32_t index, double* out);
+int mmp_batch_set_fields(mmp_batch* b, uint32_t index, const double* phi0);
+int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info);
+uint32_t mmp_batch_size(const mmp_batch* b);
+void mmp_batch_destroy(mmp_batch* b);
+
+/* ---- library facts ----------------------------------------------------------------- */
+const char* mmp_strerror(int code);
+const char* mmp_version(void);
+/* Number of this library's kernels launched so far in this process (all devices). */
+uint64_t mmp_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MMP_B200_H */
