@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""bench.py — throughput of the Lawson–RK step (mode-samples·steps/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...     (replicas, one per GPU)
+
+Workload ("grin6", the 6-mode GRIN configuration): M=6, NT=16384, 20 ps window,
+1 m, 5000 steps per solve, RK4 (--order 6 for the 7-stage tableau), Raman on,
+~60 GRIN-symmetric non-zeros; a batch of B independent solves (seeded, different
+mode power splits and phases) advanced by the same launches. One bench step is
+R Lawson–RK steps of the whole batch. value = all ranks' B*M*NT*R*K / device
+time (CUDA events on the solver's stream, max over ranks).
+
+The peak power is set where the reference's own FP64 solver is stable and
+converged at this step size (see workloads.grin6 and the accuracy block); the
+throughput per step does not depend on it.
+
+--impl reference runs the reference's own CPU solver (oracle/_ref/libmmref.so,
+built from its unmodified sources) on the host cores: one process per batch
+member, K RK steps each, all cores busy.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mode-samples·steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40, help="timed bench steps (each R RK steps)")
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--batch", type=int, default=32, help="independent solves per GPU")
+    ap.add_argument("--rk-per-step", type=int, default=50, help="RK steps per bench step")
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--peak-w", type=float, default=500.0, help="total peak power per solve (W)")
+    ap.add_argument("--fp64", action="store_true", help="all-FP64 arithmetic")
+    ap.add_argument("--e2e-iters", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=6, help="RK steps per process in the CPU sample")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
+    return ap.parse_args()
+
+
+# ---- process-group plumbing ----------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(self.local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.pg = td
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks during the timed region --------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        self.idx = gpu_index
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---- workload ------------------------------------------------------------------------------
+def make_batch_problems(args, rank: int):
+    from mm_propagation_b200 import capi, workloads as W
+    flags = capi.MMP_F_FP64 if args.fp64 else 0
+    return [W.grin6(seed=1000 * rank + i, order=args.order, peak_total_w=args.peak_w, flags=flags)
+            for i in range(args.batch)]
+
+
+def stage_bytes(prob, tab_s, a, b, bt, pairs):
+    """Algorithmic DRAM bytes per launch for each kernel kind, one solve, averaged
+    over the stages of a step (complex elements of bt bytes; psi_hat is FP64)."""
+    M, NT = prob.n_modes, prob.nt
+    P = pairs
+    pair = (M + P + 1) * NT * bt                       # read U, write W, read H_R
+    contract = (2 * M + P) * NT * bt                   # read U and W, write sigma
+    nu = 0.0
+    for i in range(tab_s):
+        last = i == tab_s - 1
+        rows = 3 * M * bt + M * 16                     # read sigma, write N_i, write U; read psi_hat
+        if last:
+            rows += M * 16 + sum(1 for j in range(tab_s) if b[j] != 0 and j != i) * M * bt
+        else:
+            rows += sum(1 for j in range(i) if a[i + 1][j] != 0) * M * bt  # N_i is in registers
+        nu += rows * NT
+    return {"pair": pair, "contract": contract, "nu": nu / tab_s}
+
+
+def read_measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_ncu_traffic(kind: str, workload: str):
+    """dram bytes per launch from the committed ncu summary, scaled to this batch."""
+    p = os.path.join(ROOT, "profiles", f"{kind}_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_solve_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+# ---- CPU side: the reference's own solver in worker processes ------------------------------
+def _ref_worker(q, spec):
+    os.environ["OMP_NUM_THREADS"] = str(spec["threads"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np  # noqa: F401
+    import ref_lib
+    from mm_propagation_b200 import workloads as W
+    prob = W.grin6(seed=spec["seed"], order=spec["order"], peak_total_w=spec["peak_w"])
+    out, sec = ref_lib.run(prob, [spec["steps"]])
+    q.put((spec["index"], sec, out if spec["keep"] else None, ref_lib.threads(prob.n_modes)))
+
+
+def run_reference_cpu(n_members: int, steps: int, order: int, peak_w: float, keep_first: bool):
+    ncpu = os.cpu_count() or 1
+    nproc = max(1, min(n_members, ncpu))
+    threads = max(1, ncpu // nproc)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = []
+    for i in range(nproc):
+        spec = {"seed": i, "order": order, "peak_w": peak_w, "steps": steps, "threads": threads,
+                "index": i, "keep": keep_first and i == 0}
+        p = ctx.Process(target=_ref_worker, args=(q, spec))
+        p.start()
+        procs.append(p)
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    secs = [r[1] for r in res]
+    first = next((r[2] for r in res if r[0] == 0), None)
+    eff_threads = res[0][3][1]
+    return {"procs": nproc, "threads_per_proc": threads, "effective_omp_threads": eff_threads,
+            "max_seconds": max(secs), "first_output": first}
+
+
+def reference_arm(args, dist):
+    if dist.rank != 0:
+        return None
+    from mm_propagation_b200 import workloads as W
+    probe = W.grin6(seed=0, order=args.order, peak_total_w=args.peak_w)
+    steps = max(1, min(args.steps, 20))
+    r = run_reference_cpu(args.batch, steps, args.order, args.peak_w, keep_first=False)
+    work = r["procs"] * probe.n_modes * probe.nt * steps
+    value = work / r["max_seconds"]
+    cores = r["procs"] * r["effective_omp_threads"]
+    sample = (f"{r['procs']} concurrent reference solves (one process each, batch members), "
+              f"{steps} RK steps each, OMP threads/process {r['threads_per_proc']} "
+              f"(reference uses {r['effective_omp_threads']})")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+        "ms_per_step": 1000.0 * r["max_seconds"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, probe, dist.world),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def workload_config(args, probe, world):
+    from mm_propagation_b200 import capi  # noqa: F401
+    nnz = int((probe.coupling["value"] != 0).sum())
+    return {"workload": f"grin6: M={probe.n_modes}, NT={probe.nt}, RK order {args.order}, Raman on, "
+                        f"{nnz} GRIN non-zeros, batch of {args.batch} independent solves per GPU",
+            "global_batch": args.batch * world, "rk_steps_per_bench_step": args.rk_per_step,
+            "peak_total_w": args.peak_w, "precision": "fp64" if args.fp64 else "fp32-bulk+fp64-phase/accum",
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (batch state > 126 MB)"}
+
+
+# ---- our arm -------------------------------------------------------------------------------
+def ours_arm(args, dist):
+    import numpy as np
+    import mm_propagation_b200 as mmp
+    from mm_propagation_b200 import capi
+
+    lib = mmp.lib()
+    probs = make_batch_problems(args, dist.rank)
+    probe = probs[0]
+    M, NT = probe.n_modes, probe.nt
+    R, K = args.rk_per_step, args.steps
+    batch = mmp.Batch(probs)
+    info = batch.info(0)
+    n_pairs = info["n_pair_fields"]
+    state_mb = sum((p.n_modes * p.nt * 16 * 2 + (p.n_stages + 2) * p.n_modes * p.nt * (16 if args.fp64 else 8)
+                    + n_pairs * p.nt * (16 if args.fp64 else 8)) for p in probs) / 1e6
+    for _ in range(args.warmup):
+        batch.propagate(R)
+    if args.profile_only:
+        batch.propagate(R)
+        return None
+    # per-kernel device times (un-graphed, one event pair per launch)
+    prof = batch.profile(2)
+    # timed region
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    clocks.start()
+    time.sleep(0.3)
+    l0 = lib.mmp_kernel_launch_count()
+    ms = batch.propagate_timed(R, K)
+    launches = lib.mmp_kernel_launch_count() - l0
+    clk = clocks.stop()
+    dist.barrier()
+    ms_max = dist.max(ms)
+    work = dist.world * args.batch * M * NT * R * K
+    value = work / (ms_max / 1000.0)
+
+    # e2e through the public API with pinned host buffers
+    import torch
+    pin_in = [torch.from_numpy(np.ascontiguousarray(p.initial_fields)).pin_memory() for p in probs]
+    pin_out = [torch.empty((p.n_modes, p.nt), dtype=torch.complex128).pin_memory() for p in probs]
+    nsteps = probe.n_steps
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_iters):
+        for i in range(len(probs)):
+            batch.set_fields(i, pin_in[i].numpy())
+        batch.propagate(nsteps)
+        for i in range(len(probs)):
+            batch.result(i, pin_out[i].numpy())
+    t_e2e = dist.max(time.perf_counter() - t0)
+    e2e_value = dist.world * args.batch * M * NT * nsteps * args.e2e_iters / t_e2e
+    h2d = sum(p.n_modes * p.nt * 16 for p in probs)
+
+    # roofline of the dominant kernel
+    bt = 16 if args.fp64 else 8
+    tab = batch_tableau(args.order)
+    per = stage_bytes(probe, tab[3], tab[0], tab[1], bt, n_pairs)
+    share = {k: prof[k]["ms_per_launch"] * prof[k]["launches"] for k in prof}
+    tot = sum(share.values())
+    dom = max(share, key=share.get)
+    peak, peak_kind = read_measured_peaks()
+    kernels = {}
+    for k in prof:
+        if not prof[k]["launches"]:
+            continue
+        bytes_launch = per[k] * args.batch
+        ach = bytes_launch / (prof[k]["ms_per_launch"] / 1e3) / 1e9
+        kernels[k] = {"ms_per_launch": prof[k]["ms_per_launch"], "share": share[k] / tot,
+                      "alg_bytes_per_launch": bytes_launch, "achieved_gbs": ach, "frac": ach / peak}
+    traffic_solve = read_ncu_traffic({"pair": "k_pair", "contract": "k_contract", "nu": "k_nu"}[dom], "grin6")
+    roof = {"bound": "hbm", "kernel": {"pair": "k_pair", "contract": "k_contract", "nu": "k_nu"}[dom],
+            "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": kernels[dom]["frac"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic_solve * args.batch if traffic_solve else None,
+            "alg_bytes_per_launch": kernels[dom]["alg_bytes_per_launch"], "kernels": kernels}
+
+    # accuracy and the CPU baseline (rank 0, N=1 only)
+    cpu = None
+    acc = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_accuracy:
+        cs = args.cpu_steps
+        r = run_reference_cpu(args.batch, cs, args.order, args.peak_w, keep_first=True)
+        cpu_value = r["procs"] * M * NT * cs / r["max_seconds"]
+        cpu = {"value": cpu_value, "unit": METRIC, "cores": r["procs"] * r["effective_omp_threads"],
+               "kind": "reference",
+               "sample": f"{r['procs']} concurrent reference solves of this workload (oracle/_ref, "
+                         f"unmodified reference sources + FFTW-API shim), {cs} RK steps each"}
+        from mm_propagation_b200 import workloads as W
+        p0 = W.grin6(seed=0, order=args.order, peak_total_w=args.peak_w)
+        acc = {}
+        for name, fl in (("fp32", 0), ("fp64", capi.MMP_F_FP64)):
+            with mmp.Solver(p0.replace(flags=fl)) as s:
+                s.propagate(cs)
+                out = s.result()
+            ref = r["first_output"]
+            err = np.sqrt((np.abs(out - ref) ** 2).sum(-1) / (np.abs(ref) ** 2).sum(-1)).max()
+            acc[f"relL2_max_{name}_vs_reference_{cs}_steps"] = float(err)
+        full = {}
+        for name, fl in (("fp32", 0), ("fp64", capi.MMP_F_FP64)):
+            with mmp.Solver(p0.replace(flags=fl)) as s:
+                s.propagate(p0.n_steps)
+                full[name] = s.result()
+        with mmp.Solver(p0.replace(flags=capi.MMP_F_FP64, n_steps=2 * p0.n_steps)) as s:
+            s.propagate(2 * p0.n_steps)
+            full["fp64_2x"] = s.result()
+
+        def rel(x, y):
+            return float(np.sqrt((np.abs(x - y) ** 2).sum(-1) / (np.abs(y) ** 2).sum(-1)).max())
+        acc["relL2_max_fp32_vs_fp64_full_solve"] = rel(full["fp32"], full["fp64"])
+        acc["relL2_max_fp64_vs_fp64_2x_steps_full_solve"] = rel(full["fp64"], full["fp64_2x"])
+        acc["tolerance"] = 1e-5
+    batch.close()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32", "data": "synthetic",
+        "config": {**workload_config(args, probe, dist.world), "state_mb_per_gpu": round(state_mb, 1)},
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+                "rk_steps_per_e2e_step": nsteps,
+                "note": "one e2e step = set_fields (pinned H2D) + a full n_steps solve + get_result (D2H) "
+                        "for every batch member, wall clock"},
+        "gpu_launches": int(launches), "clocks": clk, "accuracy": acc,
+    }
+    return line
+
+
+def batch_tableau(order):
+    """Tableau coefficients from the library (mmp_tableau) for the byte model."""
+    import mm_propagation_b200 as mmp
+    a, b, c = mmp.tableau(order)
+    a = [row + [0.0] * (len(b) - len(row)) for row in a]
+    return a, b, c, len(b)
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        line = reference_arm(args, dist) if args.impl == "reference" else ours_arm(args, dist)
+        if line is not None and dist.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,8 +170,36 @@ int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info);
 uint32_t mmp_batch_size(const mmp_batch* b);
 void mmp_batch_destroy(mmp_batch* b);
 
+/* ---- measurement (no counterpart in the reference, which has no timing code) --------- */
+/* `repeats` calls of mmp_batch_propagate_async(b, nz) bracketed by CUDA events on the
+ * batch's own stream; *ms receives the device time between the events. */
+int mmp_batch_propagate_timed(mmp_batch* b, uint32_t nz, uint32_t repeats, double* ms);
+/* nz steps launched one kernel at a time (no graph) with an event pair around every
+ * launch; ms_per_launch[kind] is the mean device time of one launch and launches[kind]
+ * the count, kind 0 = pair fields (Raman), 1 = contraction, 2 = per-mode transform
+ * kernel. Numerically identical to mmp_batch_propagate. */
+int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t* launches);
+
+/* ---- Runge–Kutta tableaus ---------------------------------------------------------- */
+/* Butcher4 / Butcher7(nu=1) / Butcher11 / Butcher7(lambda, mu) (include/RungeKutta.hpp:10-22,
+ * src/RungeKutta.cpp:3-175), selected as the solver selects them from method_order and
+ * rk_variant. Writes the stage count to *s and a (row-major 11x11, zero-padded), b[11],
+ * c[11]; any of a, b, c may be NULL. */
+int mmp_tableau(uint32_t method_order, int32_t rk_variant, double rk_lambda, double rk_mu,
+                uint32_t* s, double* a, double* b, double* c);
+
+/* ---- the transform on its own ------------------------------------------------------ */
+/* Forward_DFT::compute / Inverse_DFT::compute (include/DiscreteFourierTransform.hpp:28-45,
+ * src/DiscreteFourierTransform.cpp:24-38), batched over `rows` rows of n samples on the
+ * device, through the same FFT code the solver uses. in/out are [rows][n][2] host
+ * buffers (may alias). direction -1: unnormalised forward transform; +1: inverse scaled
+ * by 1/n, as the reference's Inverse_DFT. fp64 = 0 transforms in FP32, 1 in FP64. */
+int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in, double* out);
+
 /* ---- library facts ----------------------------------------------------------------- */
 const char* mmp_strerror(int code);
+/* Text of the last failure on the calling thread (empty when none). */
+const char* mmp_last_error(void);
 const char* mmp_version(void);
 /* Number of this library's kernels launched so far in this process (all devices). */
 uint64_t mmp_kernel_launch_count(void);

@@ -1,0 +1,214 @@
+"""mm_propagation_b200 — Lawson–Runge–Kutta multimode NLSE solver on B200 (sm_100a).
+
+Python face of the C ABI in include/mmp.h (the C++ drop-in classes live in
+include/MultimodePropagation_B200.hpp). Every computation runs in
+libmmp_b200.so's CUDA kernels; if the library or a B200 is missing, calls
+raise. There is no CPU fallback.
+
+    from mm_propagation_b200 import Solver, workloads
+    prob = workloads.grin2(peak_scale=0.01)
+    with Solver(prob) as s:
+        s.propagate(prob.n_steps)      # computeLawsonRK(n_steps)
+        phi = s.result()               # getResult(), complex128 [M][NT]
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi, workloads  # noqa: F401
+from .capi import (MMP_F_CONTINUOUS, MMP_F_FP64, MMP_F_NO_MONITORS,  # noqa: F401
+                   MMP_F_PHYSICAL_PAIRS, MMP_RK_BUTCHER7_LAMBDA_MU, MMP_RK_BY_ORDER)
+
+__all__ = ["Solver", "Batch", "MMPError", "dft", "lib", "workloads", "capi"]
+
+
+class MMPError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        l = capi.load()
+        detail = l.mmp_last_error().decode()
+        super().__init__(f"{where}: {l.mmp_strerror(code).decode()} ({code}): {detail}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    return capi.load()
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise MMPError(rc, where)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def validate(prob) -> tuple[int, str]:
+    h = prob.to_params()
+    buf = C.create_string_buffer(512)
+    rc = lib().mmp_validate_params(h.ptr(), buf, 512)
+    return rc, buf.value.decode()
+
+
+def tableau(method_order: int = 4, rk_variant: int = 0, lam: float = 0.0, mu: float = 0.0):
+    """(a, b, c) of the RK tableau the solver uses for these settings (host-side data)."""
+    s = C.c_uint32(0)
+    a = (C.c_double * 121)()
+    b = (C.c_double * 11)()
+    c = (C.c_double * 11)()
+    _check(lib().mmp_tableau(method_order, rk_variant, lam, mu, C.byref(s), a, b, c), "mmp_tableau")
+    n = s.value
+    return ([[a[i * 11 + j] for j in range(i)] for i in range(n)], list(b[:n]), list(c[:n]))
+
+
+def info_dict(info: capi.mmp_info) -> dict:
+    return {name: getattr(info, name) for name, _ in info._fields_}
+
+
+class Solver:
+    """One solve: MultimodePropagationB200_RamanOFF/ON behind the C ABI."""
+
+    def __init__(self, prob):
+        self.prob = prob
+        self._h = prob.to_params()
+        self._ptr = C.c_void_p()
+        _check(lib().mmp_solver_create(self._h.ptr(), C.byref(self._ptr)), "mmp_solver_create")
+        self.M, self.nt = prob.n_modes, prob.nt
+
+    def propagate(self, nz: int | None = None):
+        """computeLawsonRK(nz); nz=None means computeLawsonRK() (floor(z_final/dz) steps)."""
+        if nz is None:
+            _check(lib().mmp_propagate_default(self._ptr), "mmp_propagate_default")
+        else:
+            _check(lib().mmp_propagate(self._ptr, int(nz)), "mmp_propagate")
+
+    def propagate_async(self, nz: int):
+        _check(lib().mmp_propagate_async(self._ptr, int(nz)), "mmp_propagate_async")
+
+    def synchronize(self):
+        _check(lib().mmp_synchronize(self._ptr), "mmp_synchronize")
+
+    def result(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.M, self.nt), dtype=np.complex128)
+        _check(lib().mmp_get_result(self._ptr, _dptr(out.view(np.float64))), "mmp_get_result")
+        return out
+
+    def set_fields(self, phi0: np.ndarray):
+        a = np.ascontiguousarray(phi0, dtype=np.complex128)
+        _check(lib().mmp_set_fields(self._ptr, _dptr(a.view(np.float64))), "mmp_set_fields")
+
+    def monitors(self, max_steps: int | None = None):
+        info = self.info()
+        n = info["steps_done"] if max_steps is None else max_steps
+        e = np.zeros(max(n, 1))
+        p = np.zeros(max(n, 1))
+        w = C.c_uint64(0)
+        _check(lib().mmp_get_monitors(self._ptr, _dptr(e), _dptr(p), n, C.byref(w)), "mmp_get_monitors")
+        return e[:w.value], p[:w.value]
+
+    def info(self) -> dict:
+        i = capi.mmp_info()
+        _check(lib().mmp_get_info(self._ptr, C.byref(i)), "mmp_get_info")
+        return info_dict(i)
+
+    def close(self):
+        if self._ptr:
+            lib().mmp_solver_destroy(self._ptr)
+            self._ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent solves advanced together by the same launches (shared NT,
+    precision, Raman choice and RK tableau)."""
+
+    def __init__(self, probs):
+        self.probs = list(probs)
+        self._hs = [p.to_params() for p in self.probs]
+        arr = (C.POINTER(capi.mmp_params) * len(self._hs))(*[h.ptr() for h in self._hs])
+        self._ptr = C.c_void_p()
+        _check(lib().mmp_batch_create(arr, len(self._hs), C.byref(self._ptr)), "mmp_batch_create")
+
+    def __len__(self):
+        return len(self.probs)
+
+    def propagate(self, nz: int):
+        _check(lib().mmp_batch_propagate(self._ptr, int(nz)), "mmp_batch_propagate")
+
+    def propagate_async(self, nz: int):
+        _check(lib().mmp_batch_propagate_async(self._ptr, int(nz)), "mmp_batch_propagate_async")
+
+    def synchronize(self):
+        _check(lib().mmp_batch_synchronize(self._ptr), "mmp_batch_synchronize")
+
+    def propagate_timed(self, nz: int, repeats: int = 1) -> float:
+        """repeats x propagate(nz) timed with CUDA events on the batch's stream (ms)."""
+        ms = C.c_double(0.0)
+        _check(lib().mmp_batch_propagate_timed(self._ptr, int(nz), int(repeats), C.byref(ms)),
+               "mmp_batch_propagate_timed")
+        return ms.value
+
+    def profile(self, nz: int) -> dict:
+        """Per-kernel mean device time of one launch (ms) over nz un-graphed steps."""
+        ms = (C.c_double * 3)()
+        n = (C.c_uint32 * 3)()
+        _check(lib().mmp_batch_profile(self._ptr, int(nz), ms, n), "mmp_batch_profile")
+        return {k: {"ms_per_launch": ms[i], "launches": n[i]}
+                for i, k in enumerate(("pair", "contract", "nu"))}
+
+    def result(self, i: int, out: np.ndarray | None = None) -> np.ndarray:
+        p = self.probs[i]
+        if out is None:
+            out = np.empty((p.n_modes, p.nt), dtype=np.complex128)
+        _check(lib().mmp_batch_get_result(self._ptr, i, _dptr(out.view(np.float64))), "mmp_batch_get_result")
+        return out
+
+    def set_fields(self, i: int, phi0: np.ndarray):
+        a = np.ascontiguousarray(phi0, dtype=np.complex128)
+        _check(lib().mmp_batch_set_fields(self._ptr, i, _dptr(a.view(np.float64))), "mmp_batch_set_fields")
+
+    def info(self, i: int) -> dict:
+        inf = capi.mmp_info()
+        _check(lib().mmp_batch_get_info(self._ptr, i, C.byref(inf)), "mmp_batch_get_info")
+        return info_dict(inf)
+
+    def close(self):
+        if self._ptr:
+            lib().mmp_batch_destroy(self._ptr)
+            self._ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dft(x: np.ndarray, inverse: bool = False, fp64: bool = True) -> np.ndarray:
+    """Batched transform of the rows of x on the device (Forward_DFT / Inverse_DFT)."""
+    a = np.ascontiguousarray(np.atleast_2d(x), dtype=np.complex128)
+    out = np.empty_like(a)
+    rows, n = a.shape
+    _check(lib().mmp_dft(n, rows, 1 if inverse else -1, 1 if fp64 else 0, _dptr(a.view(np.float64)),
+                         _dptr(out.view(np.float64))), "mmp_dft")
+    return out.reshape(np.shape(x)) if np.ndim(x) == 1 else out

@@ -101,7 +101,15 @@ SIGNATURES = {
     "mmp_batch_get_info": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(mmp_info)]),
     "mmp_batch_size": (C.c_uint32, [C.c_void_p]),
     "mmp_batch_destroy": (None, [C.c_void_p]),
+    "mmp_batch_propagate_timed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]),
+    "mmp_batch_profile": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_uint32)]),
+    "mmp_tableau": (C.c_int, [C.c_uint32, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_uint32),
+                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "mmp_dft": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
+                         C.POINTER(C.c_double)]),
     "mmp_strerror": (C.c_char_p, [C.c_int]),
+    "mmp_last_error": (C.c_char_p, []),
     "mmp_version": (C.c_char_p, []),
     "mmp_kernel_launch_count": (C.c_uint64, []),
 }

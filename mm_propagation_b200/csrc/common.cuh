@@ -1,0 +1,116 @@
+// common.cuh — complex helpers and per-solve device descriptors shared by every kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mmp {
+
+template <typename T> struct cvec;
+template <> struct cvec<float> { using type = float2; };
+template <> struct cvec<double> { using type = double2; };
+template <typename T> using c2 = typename cvec<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ c2<T> mk(T re, T im) {
+  c2<T> r; r.x = re; r.y = im; return r;
+}
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) { a.x += b.x; a.y += b.y; return a; }
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+  V r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+// a * conj(b)
+template <typename V> __host__ __device__ __forceinline__ V cmulc(V a, V b) {
+  V r;
+  r.x = a.x * b.x + a.y * b.y;
+  r.y = a.y * b.x - a.x * b.y;
+  return r;
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) { a.y = -a.y; return a; }
+template <typename V, typename S> __host__ __device__ __forceinline__ V cscale(V a, S s) {
+  a.x *= s; a.y *= s; return a;
+}
+// multiply by i (INV=false: -i, the forward-DFT rotation; INV=true: +i)
+template <bool PLUS_I, typename V> __host__ __device__ __forceinline__ V crot(V a) {
+  V r;
+  if (PLUS_I) { r.x = -a.y; r.y = a.x; }
+  else        { r.x = a.y;  r.y = -a.x; }
+  return r;
+}
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+template <typename T> __device__ __forceinline__ c2<T> from_d2(double2 a);
+template <> __device__ __forceinline__ float2 from_d2<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 from_d2<double>(double2 a) { return a; }
+
+// Padded shared-memory index: one spare element per 32 keeps the Stockham
+// passes' strided stores free of bank conflicts for 8- and 16-byte elements.
+__host__ __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 5); }
+
+// Maximum number of RK stages (Butcher11) and dispersion orders handled.
+constexpr int kMaxStages = 11;
+constexpr int kMaxBeta = 13;
+
+// One contraction term of sigma_p = sum Q * U_k * W_pair (W conjugated when conj != 0).
+// For Raman-off solves (l, m) name the modes whose product U_l conj(U_m) is the pair field.
+struct Term {
+  int k;
+  int pair;
+  int l, m;
+  int conj;
+  int pad_;
+  double q;
+};
+
+// Everything a kernel needs about one solve. Lives in device memory (an array
+// of these per batch); kernels index it with blockIdx.y.
+struct SolveDesc {
+  int M;            // modes
+  int P;            // distinct pair fields (l <= m) formed on the device
+  int n_beta;       // polynomial coefficients per mode
+  int raman;        // 1: W = (1-fR) V + h_R (*) V; 0: W = V
+  double alpha_scale;   // 2*pi / t_final
+  double dz;            // h (dimensionless)
+  double sgn_gamma;     // +1 / -1
+  double one_minus_fR;  // 1 - f_R (Raman on)
+  double inv_nt;        // 1 / NT
+  double result_scale;  // 1 / (NT * conversion_factor)
+  double energy_scale;  // converts sum |psi_hat|^2 into pJ
+  double omega0_T0;     // dimensionless carrier, 0 disables the photon monitor
+  double photon_scale;
+  const double* poly;   // [M][n_beta]: Im L_p(alpha) = sum_j poly[p][j] alpha^j
+  double2* psi_hat;     // [M][NT] interaction-picture field, frequency domain, FP64
+  void* Nh;             // [s][M][NT] stage derivatives, frequency domain (T2)
+  void* U;              // [M][NT] stage field, time domain (T2)
+  void* W;              // [P][NT] pair fields, time domain (T2)
+  void* sigma;          // [M][NT] contraction output, time domain (T2)
+  const void* H;        // [NT] scaled Raman spectrum (T2) or null
+  double2* io;          // [M][NT] FP64 staging for upload / result
+  const int2* pairs;    // [P] (l, m)
+  const Term* terms;    // sorted by p
+  const int* term_off;  // [M+1]
+  unsigned long long* step;   // steps since the last z reset
+  unsigned long long* total;  // steps since creation (monitor index)
+  unsigned int* done_ctr;     // last-CTA counter of the final stage
+  double* energy;             // [mon_cap]
+  double* photons;            // [mon_cap]
+  unsigned long long mon_cap;
+  int* status;                // bit 0: non-finite field seen
+  int monitors;               // 1: accumulate monitors
+  int pad_;
+};
+
+// RK tableau passed by value to the stage kernels (identical for a batch).
+struct Tableau {
+  int s;
+  int last_b;                 // index of the last stage with b != 0
+  double a[kMaxStages][kMaxStages];
+  double b[kMaxStages];
+  double c[kMaxStages];
+};
+
+}  // namespace mmp

@@ -1,0 +1,1125 @@
+// solver.cu — host side of the C ABI (include/mmp.h): parameter checks, the
+// reference's setup arithmetic, device state, CUDA-graph replay of RK steps.
+//
+// The setup follows the reference's constructor step by step
+// (src/MultimodePropagation.cpp:4-56, :100-155, :165-199) in FP64 on the host;
+// everything per step runs on the device in the kernels of stage_kernels.cuh.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernel_table.h"
+#include "mmp.h"
+#include "stage_kernels.cuh"
+
+using namespace mmp;
+
+// ---------------------------------------------------------------------------------------
+// instantiated kernel sets (kern_inst.cu objects)
+#define MMP_DECL(tag, L) KernelSet make_kernels_##tag##_##L();
+#define MMP_DECL_ALL(tag) \
+  MMP_DECL(tag, 6) MMP_DECL(tag, 7) MMP_DECL(tag, 8) MMP_DECL(tag, 9) MMP_DECL(tag, 10) \
+  MMP_DECL(tag, 11) MMP_DECL(tag, 12) MMP_DECL(tag, 13) MMP_DECL(tag, 14) MMP_DECL(tag, 15) \
+  MMP_DECL(tag, 16)
+namespace mmp {
+MMP_DECL_ALL(f32)
+MMP_DECL_ALL(f64)
+
+KernelSet kernels_for(int fp64, int logn) {
+#define MMP_CASE(tag, L) case L: return make_kernels_##tag##_##L();
+  if (fp64) {
+    switch (logn) {
+      MMP_CASE(f64, 6) MMP_CASE(f64, 7) MMP_CASE(f64, 8) MMP_CASE(f64, 9) MMP_CASE(f64, 10)
+      MMP_CASE(f64, 11) MMP_CASE(f64, 12) MMP_CASE(f64, 13) MMP_CASE(f64, 14) MMP_CASE(f64, 15)
+      MMP_CASE(f64, 16)
+      default: return KernelSet();
+    }
+  }
+  switch (logn) {
+    MMP_CASE(f32, 6) MMP_CASE(f32, 7) MMP_CASE(f32, 8) MMP_CASE(f32, 9) MMP_CASE(f32, 10)
+    MMP_CASE(f32, 11) MMP_CASE(f32, 12) MMP_CASE(f32, 13) MMP_CASE(f32, 14) MMP_CASE(f32, 15)
+    MMP_CASE(f32, 16)
+    default: return KernelSet();
+  }
+#undef MMP_CASE
+}
+}  // namespace mmp
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? MMP_ENOMEM : MMP_ECUDA,              \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
+    }                                                                                    \
+  } while (0)
+
+// ---- per-device resources: twiddle tables, kernel attributes ------------------------------
+struct DeviceRes {
+  bool ready = false;
+  TwTables tw{};
+  void* tw_mem = nullptr;
+};
+std::mutex g_dev_mu;
+std::map<int, DeviceRes> g_dev;
+
+int ensure_device(int dev, DeviceRes** out) {
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceRes& r = g_dev[dev];
+  if (r.ready) { *out = &r; return MMP_OK; }
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) return fail(MMP_ENODEV, "device is not sm_100 (compute capability " +
+                                   std::to_string(prop.major) + "." + std::to_string(prop.minor) + ")");
+  // twiddle tables w_L[m] = exp(-2 pi i m / 2^L), L = 1..16, in FP64 and FP32
+  size_t n_tot = 0;
+  for (int L = 1; L <= kMaxLogN; ++L) n_tot += (size_t)1 << L;
+  std::vector<double2> hd(n_tot);
+  std::vector<float2> hf(n_tot);
+  size_t off = 0;
+  std::vector<size_t> offs(kMaxLogN + 1, 0);
+  for (int L = 1; L <= kMaxLogN; ++L) {
+    offs[L] = off;
+    const size_t n = (size_t)1 << L;
+    for (size_t m = 0; m < n; ++m) {
+      const double a = -2.0 * M_PI * (double)m / (double)n;
+      hd[off + m] = make_double2(std::cos(a), std::sin(a));
+      hf[off + m] = make_float2((float)hd[off + m].x, (float)hd[off + m].y);
+    }
+    off += n;
+  }
+  void* mem = nullptr;
+  CUDA_TRY(cudaMalloc(&mem, n_tot * (sizeof(double2) + sizeof(float2))));
+  double2* dd = (double2*)mem;
+  float2* df = (float2*)(dd + n_tot);
+  CUDA_TRY(cudaMemcpy(dd, hd.data(), n_tot * sizeof(double2), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(df, hf.data(), n_tot * sizeof(float2), cudaMemcpyHostToDevice));
+  for (int L = 0; L <= kMaxLogN; ++L) {
+    r.tw.d[L] = L ? dd + offs[L] : nullptr;
+    r.tw.f[L] = L ? df + offs[L] : nullptr;
+  }
+  r.tw_mem = mem;
+  // dynamic shared memory opt-in for every instantiated kernel
+  for (int fp64 = 0; fp64 < 2; ++fp64)
+    for (int L = kMinLogN; L <= kMaxLogN; ++L) {
+      KernelSet ks = kernels_for(fp64, L);
+      if (!ks.prime) continue;
+      const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.result, ks.dft_fwd, ks.dft_inv};
+      for (const void* f : fns)
+        CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+    }
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<double>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  r.ready = true;
+  *out = &r;
+  return MMP_OK;
+}
+
+cudaError_t launch(const void* fn, dim3 grid, int nthr, int smem, int C, cudaStream_t st, void** args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3((unsigned)nthr, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  cfg.numAttrs = 0;
+  if (C > 1) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+int ilog2_exact(uint32_t n) {
+  if (n == 0 || (n & (n - 1))) return -1;
+  int l = 0;
+  while ((1u << l) < n) ++l;
+  return l;
+}
+
+// ---- RK tableaus: src/RungeKutta.cpp ------------------------------------------------------
+void set_tableau(Tableau& t, const std::vector<std::vector<double>>& a, const std::vector<double>& b,
+                 const std::vector<double>& c) {
+  std::memset(&t, 0, sizeof(t));
+  t.s = (int)b.size();
+  for (size_t i = 0; i < a.size(); ++i)
+    for (size_t j = 0; j < a[i].size(); ++j) t.a[i][j] = a[i][j];
+  for (size_t i = 0; i < b.size(); ++i) t.b[i] = b[i];
+  for (size_t i = 0; i < (size_t)t.s; ++i) t.c[i] = c[i];
+  t.last_b = 0;
+  for (int i = 0; i < t.s; ++i)
+    if (t.b[i] != 0.0) t.last_b = i;
+}
+
+void tableau_for(const mmp_params* p, Tableau& t) {
+  const double s = std::sqrt(21.0);
+  if (p->rk_variant == MMP_RK_BUTCHER7_LAMBDA_MU) {
+    // src/RungeKutta.cpp:75-122
+    const double lam = p->rk_lambda, mu = p->rk_mu;
+    set_tableau(t,
+                {{0.},
+                 {mu},
+                 {2 / 3. - 2. / (9. * mu), 2. / (9. * mu)},
+                 {5 / 12. - 1. / (9 * mu), 1. / (9 * mu), -1 / 12.},
+                 {17 / 16. - 3. / (8. * mu), 3. / (8. * mu), -3 / 16., -3 / 8.},
+                 {17 / 16. - 3. / (8 * mu) + 1. / (4. * lam), 3. / (8. * mu), -3 / 16. - 3. / (4. * lam),
+                  -3 / 8. - 3. / (2. * lam), 2. / lam},
+                 {-27 / 44. + 3. / (11. * mu), -3. / (11. * mu), 63 / 44., 18 / 11., 4. * ((lam - 4.) / 11.),
+                  -(4. * lam) / 11.}},
+                {1 / 120., 0., 27 / 40., 27 / 40., (lam - 8.) / 15., -lam / 15., 11 / 120.},
+                {0., mu, 2 / 3., 1 / 3., 1 / 2., 1 / 2., 1.});
+    return;
+  }
+  switch (p->method_order) {
+    case 8:  // Butcher11, src/RungeKutta.cpp:125-175
+      set_tableau(
+          t,
+          {{0.},
+           {1 / 2.},
+           {1 / 4., 1 / 4.},
+           {1 / 7., (-7. + 3. * s) / 98., (21. - 5. * s) / 49.},
+           {(11. - s) / 84., 0., (18. - 4. * s) / 63., (21. + s) / 252.},
+           {(5. - s) / 48., 0., (9. - s) / 36., (-231. - 14. * s) / 360., (63. + 7. * s) / 80.},
+           {(10. + s) / 42., 0., (-432. - 92. * s) / 315., (633. + 145. * s) / 90., (-504. - 115. * s) / 70.,
+            (63. + 13. * s) / 35.},
+           {1 / 14., 0., 0., 0., (14. + 3. * s) / 126., (13. + 3. * s) / 63., 1 / 9.},
+           {1 / 32., 0., 0., 0., (91. + 21. * s) / 576., 11 / 72., (-385. + 75. * s) / 1152.,
+            (63. - 13. * s) / 128.},
+           {1 / 14., 0., 0., 0., 1 / 9., (-733. + 147. * s) / 2205., (515. - 111. * s) / 504.,
+            (-51. + 11. * s) / 56., (132. - 28. * s) / 245.},
+           {0., 0., 0., 0., (-42. - 7. * s) / 18., (-18. - 28. * s) / 45., (-273. + 53. * s) / 72.,
+            (301. - 53. * s) / 72., (28. + 28. * s) / 45., (49. + 7. * s) / 18.}},
+          {1 / 20., 0., 0., 0., 0., 0., 0., 49 / 180., 16 / 45., 49 / 180., 1 / 20.},
+          {0., 1 / 2., 1 / 2., (7. - s) / 14., (7. - s) / 14., 1 / 2., (7. + s) / 14., (7. + s) / 14., 1 / 2.,
+           (7. - s) / 14., 1.});
+      return;
+    case 6: {  // Butcher7(nu = 1), src/RungeKutta.cpp:24-72
+      const double nu = 1.0;
+      set_tableau(t,
+                  {{0.},
+                   {nu},
+                   {(4. * nu - 1.) / (8. * nu), 1. / (8. * nu)},
+                   {(10. * nu - 2.) / (27. * nu), 2. / (27. * nu), (8. * nu) / (27. * nu)},
+                   {(56. - 77. * nu + (8. - 17. * nu) * s) / (392. * nu), (-8. * (7. + s)) / (392. * nu),
+                    (48. * (7. + s) * nu) / (392. * nu), (-3. * (21. + s) * nu) / (392. * nu)},
+                   {(-5. * (287. * nu - 56. - (59. * nu - 8.) * s)) / (1960. * nu), (-40. * (7. - s)) / (1960. * nu),
+                    (320. * s * nu) / (1960. * nu), (3. * (21. - 121. * s) * nu) / (1960. * nu),
+                    (392. * (6. - s) * nu) / (1960. * nu)},
+                   {(15. * ((30. * nu - 8.) - 7. * nu * s)) / (180. * nu), 120. / (180. * nu),
+                    (-40. * (5. + 7. * s) * nu) / (180. * nu), (63. * (2. + 3. * s) * nu) / (180. * nu),
+                    (-14. * (49. - 9. * s) * nu) / (180. * nu), (70. * (7. + s) * nu) / (180. * nu)}},
+                  {9 / 180., 0., 64 / 180., 0., 49 / 180., 49 / 180., 9 / 180.},
+                  {0., nu, 1 / 2., 2 / 3., (7. + s) / 14., (7. - s) / 14., 1.});
+      return;
+    }
+    default:  // Butcher4, src/RungeKutta.cpp:3-21
+      set_tableau(t, {{0.}, {1 / 2.}, {0., 1 / 2.}, {0., 0., 1.}}, {1 / 6., 1 / 3., 1 / 3., 1 / 6.},
+                  {0., 1 / 2., 1 / 2., 1.});
+      return;
+  }
+}
+
+// ---- one solve: host setup and device buffers ---------------------------------------------
+struct Member {
+  uint32_t M = 0, nt = 0, n_beta = 0, n_steps = 0;
+  double T0 = 0, LD = 0, t_final = 0, delta_t = 0, z_final = 0, delta_z = 0, cf = 0;
+  double max_beta2 = 0, max_Q = 0, sgn_gamma = 1, fR = 0, omega0 = 0;
+  std::vector<uint32_t> unique_pairs;
+  std::vector<int2> pairs;
+  std::vector<Term> terms;
+  std::vector<int> term_off;
+  std::vector<double> poly;
+  bool quirk = false;
+  uint32_t flags = 0;
+  // device
+  void* block = nullptr;  // one allocation for all per-solve buffers
+  SolveDesc desc{};
+  unsigned long long* counters = nullptr;  // step, total, done_ctr|status
+  double* energy = nullptr;
+  double* photons = nullptr;
+  unsigned long long mon_cap = 0;
+  unsigned long long total_host = 0;  // steps enqueued since creation
+  unsigned long long step_host = 0;   // steps since the last z reset
+};
+
+int validate(const mmp_params* p, std::string& why) {
+  if (!p) { why = "params is NULL"; return MMP_EINVAL; }
+  if (p->n_modes == 0) { why = "n_modes must be >= 1"; return MMP_EINVAL; }
+  if (p->nt == 0) { why = "nt must be >= 1"; return MMP_EINVAL; }
+  if (!p->dispersion) { why = "dispersion_coefficients is NULL"; return MMP_EINVAL; }
+  if (p->n_beta < 3) {
+    why = "dispersion_coefficients needs >= 3 orders per mode (beta[p][2] is read, src/MultimodePropagation.cpp:71)";
+    return MMP_EINVAL;
+  }
+  if (p->n_beta > (uint32_t)kMaxBeta) { why = "at most 13 dispersion orders (int factorial of the reference overflows beyond 12!)"; return MMP_EINVAL; }
+  if (!p->initial_fields) { why = "initial_fields is NULL"; return MMP_EINVAL; }
+  if (p->n_nonzeros && !p->coupling) { why = "coupling is NULL with n_nonzeros > 0"; return MMP_EINVAL; }
+  if (!(p->pulse_width > 0) || !std::isfinite(p->pulse_width)) { why = "pulse_width must be > 0"; return MMP_EINVAL; }
+  if (!(p->time_window > 0) || !std::isfinite(p->time_window)) { why = "time_window must be > 0"; return MMP_EINVAL; }
+  if (!(p->fiber_length > 0) || !std::isfinite(p->fiber_length)) { why = "fiber_length must be > 0"; return MMP_EINVAL; }
+  if (p->n_steps == 0) { why = "n_steps must be >= 1"; return MMP_EINVAL; }
+  if (!std::isfinite(p->nonlinearity_const)) { why = "nonlinearity_const must be finite"; return MMP_EINVAL; }
+  double mb2 = 0, mq = 0;
+  for (uint32_t m = 0; m < p->n_modes; ++m) {
+    for (uint32_t i = 0; i < p->n_beta; ++i)
+      if (!std::isfinite(p->dispersion[m * p->n_beta + i])) { why = "dispersion coefficient not finite"; return MMP_EINVAL; }
+    mb2 = std::max(mb2, std::fabs(p->dispersion[m * p->n_beta + 2]));
+  }
+  if (mb2 == 0) { why = "max |beta2| is 0: the reference's dispersion length T0^2/max|beta2| is infinite"; return MMP_EINVAL; }
+  for (uint32_t j = 0; j < p->n_nonzeros; ++j) {
+    const mmp_nz& e = p->coupling[j];
+    if (e.p >= p->n_modes || e.k >= p->n_modes || e.l >= p->n_modes || e.m >= p->n_modes) {
+      why = "coupling index out of range (entry " + std::to_string(j) + ")";
+      return MMP_EINVAL;
+    }
+    if (!std::isfinite(e.value)) { why = "coupling value not finite (entry " + std::to_string(j) + ")"; return MMP_EINVAL; }
+    mq = std::max(mq, std::fabs(e.value));
+  }
+  if (mq == 0) { why = "max |Q| is 0: the reference divides Q by it (src/MultimodePropagation.cpp:117-136)"; return MMP_EINVAL; }
+  if (p->raman) {
+    if (!p->raman_response) { why = "raman_response is NULL for a Raman-on solver"; return MMP_EINVAL; }
+    if (!std::isfinite(p->raman_proportion)) { why = "raman_proportion not finite"; return MMP_EINVAL; }
+    for (uint32_t t = 0; t < p->nt; ++t)
+      if (!std::isfinite(p->raman_response[t])) { why = "raman_response not finite"; return MMP_EINVAL; }
+  }
+  for (size_t t = 0; t < 2 * (size_t)p->n_modes * p->nt; ++t)
+    if (!std::isfinite(p->initial_fields[t])) { why = "initial_fields not finite"; return MMP_EINVAL; }
+  if (p->rk_variant == MMP_RK_BUTCHER7_LAMBDA_MU && (p->rk_lambda == 0 || p->rk_mu == 0)) {
+    why = "Butcher7(lambda, mu) needs lambda != 0 and mu != 0"; return MMP_EINVAL;
+  }
+  if (p->rk_variant != MMP_RK_BY_ORDER && p->rk_variant != MMP_RK_BUTCHER7_LAMBDA_MU) {
+    why = "unknown rk_variant"; return MMP_EINVAL;
+  }
+  const int lg = ilog2_exact(p->nt);
+  if (lg < kMinLogN || lg > kMaxLogN) {
+    why = "nt must be a power of two in [64, 65536] in this build";
+    return MMP_ENOTSUP;
+  }
+  return MMP_OK;
+}
+
+// The reference's setup, in FP64 with the same expressions.
+void host_setup(const mmp_params* p, Member& s) {
+  const uint32_t M = p->n_modes, L = p->n_beta;
+  s.M = M; s.nt = p->nt; s.n_beta = L; s.n_steps = p->n_steps; s.flags = p->flags;
+  s.T0 = p->pulse_width;
+  const double gamma = p->nonlinearity_const;
+  s.sgn_gamma = gamma >= 0 ? 1.0 : -1.0;                              // :34
+  double max_beta2 = 0;                                                // :67-77
+  for (uint32_t q = 0; q < M; ++q) max_beta2 = std::max(max_beta2, std::fabs(p->dispersion[q * L + 2]));
+  double max_Q = 0;                                                    // :81-97
+  for (uint32_t j = 0; j < p->n_nonzeros; ++j) max_Q = std::max(max_Q, std::fabs(p->coupling[j].value));
+  s.max_beta2 = max_beta2;
+  s.max_Q = max_Q;
+  s.LD = (s.T0 * s.T0) / max_beta2;                                    // :42
+  std::vector<double> c(L);
+  for (uint32_t i = 0; i < L; ++i) c[i] = 1. / std::pow(s.T0, (double)i) * s.LD;  // :100-106
+  s.t_final = p->time_window / s.T0;                                   // :47-48
+  s.delta_t = s.t_final / s.nt;
+  s.z_final = p->fiber_length / s.LD;                                  // :50-51
+  s.delta_z = s.z_final / p->n_steps;
+  s.cf = std::sqrt(std::fabs(gamma) * s.LD) * std::sqrt(max_Q);        // :53
+  s.fR = p->raman ? p->raman_proportion : 0.0;
+  s.omega0 = p->center_frequency;
+  // Im L_p(alpha) = bt0 - bt1 alpha - bt2/2 alpha^2 + sum_{k>=3} (-1)^k bt_k/k! alpha^k (:165-187)
+  s.poly.assign((size_t)M * L, 0.0);
+  for (uint32_t q = 0; q < M; ++q) {
+    for (uint32_t i = 0; i < L; ++i) {
+      const double bt = p->dispersion[q * L + i] * c[i];
+      double coef;
+      if (i == 0) coef = bt;
+      else if (i == 1) coef = -bt;
+      else if (i == 2) coef = -bt / 2;
+      else {
+        double fact = 1;
+        for (uint32_t f = 2; f <= i; ++f) fact *= f;
+        coef = ((i % 2) ? -1.0 : 1.0) * bt / fact;
+      }
+      s.poly[q * L + i] = coef;
+    }
+  }
+  // unique_pairs: p outer, insertion order inner (:139-155)
+  std::vector<std::vector<const mmp_nz*>> byp(M);
+  for (uint32_t j = 0; j < p->n_nonzeros; ++j) byp[p->coupling[j].p].push_back(&p->coupling[j]);
+  std::map<uint32_t, uint32_t> slot_of;
+  for (uint32_t q = 0; q < M; ++q)
+    for (const mmp_nz* e : byp[q]) {
+      const uint32_t code = e->l + e->m * M;
+      if (!slot_of.count(code)) {
+        slot_of[code] = (uint32_t)s.unique_pairs.size();
+        s.unique_pairs.push_back(code);
+      }
+    }
+  const bool physical = (p->flags & MMP_F_PHYSICAL_PAIRS) != 0;
+  s.quirk = false;
+  for (size_t i = 0; i < s.unique_pairs.size(); ++i)
+    if (s.unique_pairs[i] != i) s.quirk = !physical;
+  // contraction terms with the pair each one actually reads
+  // (reference CPU: V[slot] = U[slot % M] conj(U[slot / M]), :126-133, :195-205)
+  std::map<std::pair<int, int>, int> pair_idx;
+  s.term_off.assign(M + 1, 0);
+  for (uint32_t q = 0; q < M; ++q) {
+    s.term_off[q] = (int)s.terms.size();
+    for (const mmp_nz* e : byp[q]) {
+      if (e->value == 0.0) continue;  // contributes exactly 0
+      const uint32_t code = e->l + e->m * M;
+      const uint32_t src = physical ? code : slot_of[code];
+      const int le = (int)(src % M), me = (int)(src / M);
+      const int lo = std::min(le, me), hi = std::max(le, me);
+      auto key = std::make_pair(lo, hi);
+      if (!pair_idx.count(key)) {
+        pair_idx[key] = (int)s.pairs.size();
+        s.pairs.push_back(make_int2(lo, hi));
+      }
+      Term t;
+      t.k = (int)e->k;
+      t.pair = pair_idx[key];
+      t.l = le;
+      t.m = me;
+      t.conj = le > me ? 1 : 0;  // W_ml = conj(W_lm): h_R is real
+      t.pad_ = 0;
+      t.q = e->value / max_Q;  // Q_tilde (:117-136)
+      s.terms.push_back(t);
+    }
+  }
+  s.term_off[M] = (int)s.terms.size();
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+struct mmp_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool fp64 = false, raman = false;
+  uint32_t nt = 0;
+  int logn = 0;
+  Tableau tab{};
+  std::vector<Member> members;
+  SolveDesc* d_descs = nullptr;
+  int Mmax = 0, Pmax = 0;
+  int TT = 32;
+  size_t contract_smem = 0;
+  KernelSet ks{}, ks64{};
+  DeviceRes* dev = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int kernels_per_step = 0;
+};
+
+struct mmp_solver {
+  mmp_batch* b = nullptr;
+};
+
+namespace {
+
+void* T2ptr(void* base, size_t off) { return (char*)base + off; }
+
+int upload_desc(mmp_batch* b) {
+  std::vector<SolveDesc> h(b->members.size());
+  for (size_t i = 0; i < b->members.size(); ++i) h[i] = b->members[i].desc;
+  CUDA_TRY(cudaMemcpyAsync(b->d_descs, h.data(), h.size() * sizeof(SolveDesc), cudaMemcpyHostToDevice,
+                           b->stream));
+  return MMP_OK;
+}
+
+int grow_monitors(mmp_batch* b, Member& s, unsigned long long need) {
+  if (need <= s.mon_cap) return MMP_OK;
+  unsigned long long cap = std::max<unsigned long long>(need, s.mon_cap * 2);
+  cap = std::max<unsigned long long>(cap, 1024);
+  double* mem = nullptr;
+  CUDA_TRY(cudaMalloc(&mem, 2 * cap * sizeof(double)));
+  CUDA_TRY(cudaMemsetAsync(mem, 0, 2 * cap * sizeof(double), b->stream));
+  if (s.mon_cap) {
+    CUDA_TRY(cudaMemcpyAsync(mem, s.energy, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    CUDA_TRY(cudaMemcpyAsync(mem + cap, s.photons, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice,
+                             b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    CUDA_TRY(cudaFree(s.energy));
+  }
+  s.energy = mem;
+  s.photons = mem + cap;
+  s.mon_cap = cap;
+  s.desc.energy = s.energy;
+  s.desc.photons = s.photons;
+  s.desc.mon_cap = cap;
+  return upload_desc(b);
+}
+
+// launch helpers ------------------------------------------------------------------------
+KParams kparams(mmp_batch* b, int stage, const SolveDesc* descs) {
+  KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.descs = descs;
+  kp.tw = b->dev->tw;
+  kp.tab = b->tab;
+  kp.stage = stage;
+  return kp;
+}
+
+int launch_row_kernel(mmp_batch* b, const KernelSet& ks, const void* fn, int rows, int nsolves, int stage,
+                      const SolveDesc* descs) {
+  if (rows <= 0) return MMP_OK;
+  KParams kp = kparams(b, stage, descs);
+  void* args[] = {&kp};
+  dim3 grid((unsigned)(rows * ks.C), (unsigned)nsolves, 1);
+  CUDA_TRY(launch(fn, grid, ks.nthr, ks.smem, ks.C, b->stream, args));
+  return MMP_OK;
+}
+
+int launch_contract(mmp_batch* b) {
+  const SolveDesc* descs = b->d_descs;
+  int nt = (int)b->nt, TT = b->TT;
+  void* args[] = {(void*)&descs, &nt, &TT};
+  dim3 grid((unsigned)(b->nt / b->TT), (unsigned)b->members.size(), 1);
+  const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
+  CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, b->stream, args));
+  return MMP_OK;
+}
+
+int enqueue_step(mmp_batch* b) {
+  const int nsol = (int)b->members.size();
+  for (int i = 0; i < b->tab.s; ++i) {
+    int rc;
+    if (b->raman && b->Pmax > 0) {
+      rc = launch_row_kernel(b, b->ks, b->ks.pair, b->Pmax, nsol, i, b->d_descs);
+      if (rc) return rc;
+    }
+    rc = launch_contract(b);
+    if (rc) return rc;
+    rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, nsol, i, b->d_descs);
+    if (rc) return rc;
+  }
+  return MMP_OK;
+}
+
+int build_graph(mmp_batch* b, int steps) {
+  if (b->graph && b->graph_steps == steps) return MMP_OK;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  const uint64_t counted = g_launches.load();
+  CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = MMP_OK;
+  for (int k = 0; k < steps && rc == MMP_OK; ++k) rc = enqueue_step(b);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  g_launches.store(counted);  // captured launches run (and are counted) at replay
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(MMP_ECUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(MMP_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  b->graph_steps = steps;
+  return MMP_OK;
+}
+
+int check_status(mmp_batch* b) {
+  int bad = 0;
+  for (auto& s : b->members) {
+    int st = 0;
+    CUDA_TRY(cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
+                        cudaMemcpyDeviceToHost));
+    if (st & 1) bad = 1;
+  }
+  if (bad) return fail(MMP_ENONFINITE, "the field became NaN/Inf during propagation");
+  return MMP_OK;
+}
+
+int batch_propagate_async(mmp_batch* b, uint32_t nz) {
+  if (!b) return fail(MMP_EINVAL, "NULL batch");
+  CUDA_TRY(cudaSetDevice(b->device));
+  for (auto& s : b->members) {
+    const bool continuous = (s.flags & MMP_F_CONTINUOUS) != 0;
+    if (!continuous) {
+      // initLawsonRK: z = 0 (src/MultimodePropagation.cpp:158-163)
+      CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), b->stream));
+      s.step_host = 0;
+    }
+    if (!(s.flags & MMP_F_NO_MONITORS)) {
+      int rc = grow_monitors(b, s, s.total_host + nz);
+      if (rc) return rc;
+    }
+  }
+  if (nz == 0) return MMP_OK;
+  // U for stage 0 at the current z
+  int rc = launch_row_kernel(b, b->ks, b->ks.prime, b->Mmax, (int)b->members.size(), 0, b->d_descs);
+  if (rc) return rc;
+  const int G = 8;  // steps per captured graph
+  uint32_t left = nz;
+  if (left >= (uint32_t)G) {
+    rc = build_graph(b, G);
+    if (rc) return rc;
+    while (left >= (uint32_t)G) {
+      CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+      g_launches.fetch_add((uint64_t)G * b->kernels_per_step, std::memory_order_relaxed);
+      left -= G;
+    }
+  }
+  for (uint32_t k = 0; k < left; ++k) {
+    rc = enqueue_step(b);
+    if (rc) return rc;
+  }
+  for (auto& s : b->members) {
+    s.total_host += nz;
+    s.step_host += nz;
+  }
+  return MMP_OK;
+}
+
+int batch_sync(mmp_batch* b) {
+  CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return check_status(b);
+}
+
+int member_result(mmp_batch* b, uint32_t idx, double* out) {
+  if (!b || idx >= b->members.size() || !out) return fail(MMP_EINVAL, "bad result arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  Member& s = b->members[idx];
+  int rc = launch_row_kernel(b, b->ks64, b->ks64.result, (int)s.M, 1, 0, b->d_descs + idx);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(out, s.desc.io, (size_t)s.M * s.nt * sizeof(double2), cudaMemcpyDeviceToHost,
+                           b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return MMP_OK;
+}
+
+int member_set_fields(mmp_batch* b, uint32_t idx, const double* phi0) {
+  if (!b || idx >= b->members.size() || !phi0) return fail(MMP_EINVAL, "bad set_fields arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  Member& s = b->members[idx];
+  for (size_t t = 0; t < 2 * (size_t)s.M * s.nt; ++t)
+    if (!std::isfinite(phi0[t])) return fail(MMP_EINVAL, "initial fields not finite");
+  const size_t bytes = (size_t)s.M * s.nt * sizeof(double2);
+  CUDA_TRY(cudaMemcpyAsync(s.desc.io, phi0, bytes, cudaMemcpyHostToDevice, b->stream));
+  // psi_hat = FFT(cf * phi0)   (src/MultimodePropagation.cpp:59-63 in the frequency domain)
+  DftArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.in = s.desc.io;
+  a.out = s.desc.psi_hat;
+  a.rows = (int)s.M;
+  a.scale = s.cf;
+  a.tw = b->dev->tw;
+  void* args[] = {&a};
+  CUDA_TRY(launch(b->ks64.dft_fwd, dim3((unsigned)(s.M * b->ks64.C), 1, 1), b->ks64.nthr, b->ks64.smem,
+                  b->ks64.C, b->stream, args));
+  CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), b->stream));  // z = 0
+  CUDA_TRY(cudaMemsetAsync((char*)s.counters + 3 * sizeof(unsigned long long), 0, sizeof(int), b->stream));
+  s.step_host = 0;
+  return MMP_OK;
+}
+
+int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
+  if (!out) return fail(MMP_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!params || n == 0) return fail(MMP_EINVAL, "empty batch");
+  for (uint32_t i = 0; i < n; ++i) {
+    std::string why;
+    int rc = validate(params[i], why);
+    if (rc) return fail(rc, "member " + std::to_string(i) + ": " + why);
+  }
+  const mmp_params* p0 = params[0];
+  Tableau tab0;
+  tableau_for(p0, tab0);
+  for (uint32_t i = 1; i < n; ++i) {
+    const mmp_params* p = params[i];
+    Tableau t;
+    tableau_for(p, t);
+    if (p->nt != p0->nt || (p->flags & MMP_F_FP64) != (p0->flags & MMP_F_FP64) ||
+        (p->raman != 0) != (p0->raman != 0) || std::memcmp(&t, &tab0, sizeof(t)) != 0)
+      return fail(MMP_EINVAL, "batch members must share nt, precision, raman and the RK tableau");
+  }
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  DeviceRes* res = nullptr;
+  int rc = ensure_device(dev, &res);
+  if (rc) return rc;
+
+  mmp_batch* b = new mmp_batch();
+  b->device = dev;
+  b->dev = res;
+  b->fp64 = (p0->flags & MMP_F_FP64) != 0;
+  b->raman = p0->raman != 0;
+  b->nt = p0->nt;
+  b->logn = ilog2_exact(p0->nt);
+  b->tab = tab0;
+  b->ks = kernels_for(b->fp64 ? 1 : 0, b->logn);
+  b->ks64 = kernels_for(1, b->logn);
+  if (!b->ks.prime || !b->ks64.prime) {
+    delete b;
+    return fail(MMP_ENOTSUP, "no kernels built for this nt");
+  }
+  b->kernels_per_step = b->tab.s * ((b->raman ? 1 : 0) + 2);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(MMP_ECUDA, cudaGetErrorString(e));
+  }
+  b->members.resize(n);
+  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+  const size_t nt = b->nt;
+  int build_rc = MMP_OK;
+  for (uint32_t i = 0; i < n && build_rc == MMP_OK; ++i) {
+    Member& s = b->members[i];
+    host_setup(params[i], s);
+    const size_t M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
+    // one allocation: psi_hat | io | Nh | U | sigma | W | H | poly | pairs | terms | term_off | counters
+    size_t off = 0;
+    const size_t o_psi = off; off = align_up(off + M * nt * sizeof(double2));
+    const size_t o_io = off; off = align_up(off + M * nt * sizeof(double2));
+    const size_t o_nh = off; off = align_up(off + S * M * nt * t2);
+    const size_t o_u = off; off = align_up(off + M * nt * t2);
+    const size_t o_sig = off; off = align_up(off + M * nt * t2);
+    const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
+    const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
+    const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
+    const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
+    const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
+    const size_t o_toff = off; off = align_up(off + (M + 1) * sizeof(int));
+    const size_t o_cnt = off; off = align_up(off + 4 * sizeof(unsigned long long));
+    e = cudaMalloc(&s.block, off);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ENOMEM, "cudaMalloc solver state: " + std::string(cudaGetErrorString(e))); break; }
+    e = cudaMemsetAsync(s.block, 0, off, b->stream);
+    SolveDesc& d = s.desc;
+    std::memset(&d, 0, sizeof(d));
+    d.M = (int)M;
+    d.P = (int)P;
+    d.n_beta = (int)s.n_beta;
+    d.raman = b->raman ? 1 : 0;
+    d.alpha_scale = 2 * M_PI / s.t_final;
+    d.dz = s.delta_z;
+    d.sgn_gamma = s.sgn_gamma;
+    d.one_minus_fR = b->raman ? (1.0 - s.fR) : 1.0;
+    d.inv_nt = 1.0 / (double)nt;
+    d.result_scale = 1.0 / ((double)nt * s.cf);
+    d.energy_scale = s.delta_t * s.T0 / (s.cf * s.cf * (double)nt);
+    d.omega0_T0 = s.omega0 * s.T0;
+    d.photon_scale = d.energy_scale * s.T0 / 1.054571817e-10;
+    d.poly = (const double*)T2ptr(s.block, o_poly);
+    d.psi_hat = (double2*)T2ptr(s.block, o_psi);
+    d.io = (double2*)T2ptr(s.block, o_io);
+    d.Nh = T2ptr(s.block, o_nh);
+    d.U = T2ptr(s.block, o_u);
+    d.sigma = T2ptr(s.block, o_sig);
+    d.W = T2ptr(s.block, o_w);
+    d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
+    d.pairs = (const int2*)T2ptr(s.block, o_pairs);
+    d.terms = (const Term*)T2ptr(s.block, o_terms);
+    d.term_off = (const int*)T2ptr(s.block, o_toff);
+    s.counters = (unsigned long long*)T2ptr(s.block, o_cnt);
+    d.step = s.counters;
+    d.total = s.counters + 1;
+    d.done_ctr = (unsigned int*)(s.counters + 2);
+    d.status = (int*)(s.counters + 3);
+    d.monitors = (s.flags & MMP_F_NO_MONITORS) ? 0 : 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)d.poly, s.poly.data(), s.poly.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess && P) e = cudaMemcpyAsync((void*)d.pairs, s.pairs.data(), P * sizeof(int2), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess && !s.terms.empty()) e = cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    b->Mmax = std::max(b->Mmax, (int)M);
+    b->Pmax = std::max(b->Pmax, (int)(b->raman ? P : 0));
+  }
+  if (build_rc == MMP_OK) {
+    e = cudaMalloc(&b->d_descs, n * sizeof(SolveDesc));
+    if (e != cudaSuccess) build_rc = fail(MMP_ENOMEM, cudaGetErrorString(e));
+  }
+  if (build_rc == MMP_OK) build_rc = upload_desc(b);
+  // Raman spectrum: H = FFT(h_R) * dt * T0 * fR / NT  (src/MultimodePropagation_CPU.cpp:170-176, :241-251)
+  for (uint32_t i = 0; i < n && build_rc == MMP_OK && b->raman; ++i) {
+    Member& s = b->members[i];
+    std::vector<double2> hr(nt);
+    for (size_t t = 0; t < nt; ++t) hr[t] = make_double2(params[i]->raman_response[t], 0.0);
+    double2* tmp = s.desc.io;  // staging
+    double2* h64 = (double2*)s.desc.Nh;  // FP64 spectrum scratch (Nh is large enough and unused yet)
+    e = cudaMemcpyAsync(tmp, hr.data(), nt * sizeof(double2), cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    DftArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = tmp;
+    a.out = h64;
+    a.rows = 1;
+    a.scale = s.delta_t * s.T0 * s.fR / (double)nt;
+    a.tw = b->dev->tw;
+    void* args[] = {&a};
+    e = launch(b->ks64.dft_fwd, dim3((unsigned)b->ks64.C, 1, 1), b->ks64.nthr, b->ks64.smem, b->ks64.C, b->stream, args);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    const void* conv = b->fp64 ? (const void*)&k_to_t2<double> : (const void*)&k_to_t2<float>;
+    const double2* cin = h64;
+    void* cout_ = (void*)s.desc.H;
+    size_t cnt = nt;
+    void* cargs[] = {(void*)&cin, &cout_, &cnt};
+    e = launch(conv, dim3(64, 1, 1), 256, 0, 1, b->stream, cargs);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    e = cudaMemsetAsync(s.desc.Nh, 0, (size_t)b->tab.s * s.M * nt * t2, b->stream);
+    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+  }
+  for (uint32_t i = 0; i < n && build_rc == MMP_OK; ++i)
+    build_rc = member_set_fields(b, i, params[i]->initial_fields);
+  if (build_rc == MMP_OK) {
+    // contraction tile: the largest power of two <= 256 whose U+W tile fits in 100 KB
+    const int rows = b->Mmax + b->Pmax;
+    int TT = 256;
+    while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
+    while (TT > 1 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;
+    while (TT > (int)nt) TT >>= 1;
+    b->TT = TT;
+    b->contract_smem = (size_t)rows * TT * t2;
+    e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) build_rc = fail(MMP_ECUDA, cudaGetErrorString(e));
+  }
+  if (build_rc != MMP_OK) {
+    mmp_batch_destroy(b);
+    return build_rc;
+  }
+  *out = b;
+  return MMP_OK;
+}
+
+void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
+  std::memset(info, 0, sizeof(*info));
+  info->n_modes = s.M;
+  info->nt = s.nt;
+  info->n_stages = (uint32_t)b->tab.s;
+  info->n_pairs = (uint32_t)s.unique_pairs.size();
+  info->n_pair_fields = (uint32_t)s.pairs.size();
+  info->pair_quirk_active = s.quirk ? 1u : 0u;
+  info->t_final = s.t_final;
+  info->delta_t = s.delta_t;
+  info->z_final = s.z_final;
+  info->delta_z = s.delta_z;
+  info->z = (double)s.step_host * s.delta_z;
+  info->LD = s.LD;
+  info->conversion_factor = s.cf;
+  info->max_beta2 = s.max_beta2;
+  info->max_Q = s.max_Q;
+  info->steps_done = s.total_host;
+  info->fp64 = b->fp64 ? 1u : 0u;
+  info->cluster_ctas = (uint32_t)b->ks.C;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+extern "C" {
+
+int mmp_validate_params(const mmp_params* params, char* msg, size_t msg_len) {
+  std::string why;
+  int rc = validate(params, why);
+  if (msg && msg_len) {
+    std::snprintf(msg, msg_len, "%s", rc ? why.c_str() : "");
+  }
+  if (rc) g_last_error = why;
+  return rc;
+}
+
+int mmp_batch_create(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
+  return create_batch(params, n, out);
+}
+
+int mmp_batch_propagate_async(mmp_batch* b, uint32_t nz) { return batch_propagate_async(b, nz); }
+
+int mmp_batch_synchronize(mmp_batch* b) {
+  if (!b) return fail(MMP_EINVAL, "NULL batch");
+  return batch_sync(b);
+}
+
+int mmp_batch_propagate(mmp_batch* b, uint32_t nz) {
+  int rc = batch_propagate_async(b, nz);
+  if (rc) return rc;
+  return batch_sync(b);
+}
+
+int mmp_batch_get_result(mmp_batch* b, uint32_t index, double* out) { return member_result(b, index, out); }
+
+int mmp_batch_set_fields(mmp_batch* b, uint32_t index, const double* phi0) {
+  int rc = member_set_fields(b, index, phi0);
+  if (rc) return rc;
+  return MMP_OK;
+}
+
+int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info) {
+  if (!b || index >= b->members.size() || !info) return fail(MMP_EINVAL, "bad info arguments");
+  fill_info(b, b->members[index], info);
+  return MMP_OK;
+}
+
+uint32_t mmp_batch_size(const mmp_batch* b) { return b ? (uint32_t)b->members.size() : 0u; }
+
+int mmp_batch_propagate_timed(mmp_batch* b, uint32_t nz, uint32_t repeats, double* ms) {
+  if (!b || !ms) return fail(MMP_EINVAL, "bad timed-propagate arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int rc = MMP_OK;
+  cudaError_t e = cudaEventRecord(e0, b->stream);
+  for (uint32_t r = 0; r < repeats && rc == MMP_OK && e == cudaSuccess; ++r) rc = batch_propagate_async(b, nz);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float f = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(MMP_ECUDA, cudaGetErrorString(e));
+  *ms = f;
+  return check_status(b);
+}
+
+int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t* launches) {
+  if (!b || !ms_per_launch || !launches) return fail(MMP_EINVAL, "bad profile arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  for (int k = 0; k < 3; ++k) { ms_per_launch[k] = 0.0; launches[k] = 0; }
+  for (auto& s : b->members) {
+    if (!(s.flags & MMP_F_CONTINUOUS)) {
+      CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), b->stream));
+      s.step_host = 0;
+    }
+    if (!(s.flags & MMP_F_NO_MONITORS)) {
+      int rc = grow_monitors(b, s, s.total_host + nz);
+      if (rc) return rc;
+    }
+  }
+  const int nsol = (int)b->members.size();
+  int rc = launch_row_kernel(b, b->ks, b->ks.prime, b->Mmax, nsol, 0, b->d_descs);
+  if (rc) return rc;
+  cudaEvent_t ev[2];
+  CUDA_TRY(cudaEventCreate(&ev[0]));
+  CUDA_TRY(cudaEventCreate(&ev[1]));
+  double acc[3] = {0, 0, 0};
+  for (uint32_t n = 0; n < nz && rc == MMP_OK; ++n) {
+    for (int i = 0; i < b->tab.s && rc == MMP_OK; ++i) {
+      for (int kind = 0; kind < 3 && rc == MMP_OK; ++kind) {
+        if (kind == 0 && !(b->raman && b->Pmax > 0)) continue;
+        cudaError_t e = cudaEventRecord(ev[0], b->stream);
+        if (e != cudaSuccess) { rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+        if (kind == 0) rc = launch_row_kernel(b, b->ks, b->ks.pair, b->Pmax, nsol, i, b->d_descs);
+        else if (kind == 1) rc = launch_contract(b);
+        else rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, nsol, i, b->d_descs);
+        if (rc) break;
+        e = cudaEventRecord(ev[1], b->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+        float f = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&f, ev[0], ev[1]);
+        if (e != cudaSuccess) { rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+        acc[kind] += f;
+        launches[kind] += 1;
+      }
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (rc) return rc;
+  for (auto& s : b->members) {
+    s.total_host += nz;
+    s.step_host += nz;
+  }
+  for (int k = 0; k < 3; ++k) ms_per_launch[k] = launches[k] ? acc[k] / launches[k] : 0.0;
+  return batch_sync(b);
+}
+
+void mmp_batch_destroy(mmp_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto& s : b->members) {
+    if (s.block) cudaFree(s.block);
+    if (s.energy) cudaFree(s.energy);
+  }
+  if (b->d_descs) cudaFree(b->d_descs);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int mmp_solver_create(const mmp_params* params, mmp_solver** out) {
+  if (!out) return fail(MMP_EINVAL, "out is NULL");
+  *out = nullptr;
+  const mmp_params* arr[1] = {params};
+  mmp_batch* b = nullptr;
+  int rc = create_batch(arr, 1, &b);
+  if (rc) return rc;
+  mmp_solver* s = new mmp_solver();
+  s->b = b;
+  *out = s;
+  return MMP_OK;
+}
+
+int mmp_propagate(mmp_solver* s, uint32_t nz) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  return mmp_batch_propagate(s->b, nz);
+}
+
+int mmp_propagate_async(mmp_solver* s, uint32_t nz) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  return batch_propagate_async(s->b, nz);
+}
+
+int mmp_synchronize(mmp_solver* s) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  return batch_sync(s->b);
+}
+
+int mmp_propagate_default(mmp_solver* s) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  const Member& m = s->b->members[0];
+  // src/MultimodePropagation.cpp:213-216
+  const unsigned nz = (unsigned)std::floor(m.z_final / m.delta_z);
+  return mmp_batch_propagate(s->b, nz);
+}
+
+int mmp_get_result(mmp_solver* s, double* out) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  return member_result(s->b, 0, out);
+}
+
+int mmp_set_fields(mmp_solver* s, const double* phi0) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  int rc = member_set_fields(s->b, 0, phi0);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s->b->stream));
+  return MMP_OK;
+}
+
+int mmp_get_monitors(mmp_solver* s, double* energy, double* photons, uint64_t max_steps, uint64_t* n_written) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  mmp_batch* b = s->b;
+  Member& m = b->members[0];
+  CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  uint64_t n = std::min<uint64_t>(max_steps, std::min<uint64_t>(m.total_host, m.mon_cap));
+  if (m.flags & MMP_F_NO_MONITORS) n = 0;
+  if (n && energy) CUDA_TRY(cudaMemcpy(energy, m.energy, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (n && photons) CUDA_TRY(cudaMemcpy(photons, m.photons, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (n_written) *n_written = n;
+  return MMP_OK;
+}
+
+int mmp_get_info(mmp_solver* s, mmp_info* info) {
+  if (!s || !info) return fail(MMP_EINVAL, "bad info arguments");
+  fill_info(s->b, s->b->members[0], info);
+  return MMP_OK;
+}
+
+void mmp_solver_destroy(mmp_solver* s) {
+  if (!s) return;
+  mmp_batch_destroy(s->b);
+  delete s;
+}
+
+int mmp_tableau(uint32_t method_order, int32_t rk_variant, double rk_lambda, double rk_mu, uint32_t* s,
+                double* a, double* b, double* c) {
+  if (rk_variant != MMP_RK_BY_ORDER && rk_variant != MMP_RK_BUTCHER7_LAMBDA_MU)
+    return fail(MMP_EINVAL, "unknown rk_variant");
+  mmp_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.method_order = method_order;
+  p.rk_variant = rk_variant;
+  p.rk_lambda = rk_lambda;
+  p.rk_mu = rk_mu;
+  Tableau t;
+  tableau_for(&p, t);
+  if (s) *s = (uint32_t)t.s;
+  for (int i = 0; i < kMaxStages; ++i) {
+    for (int j = 0; j < kMaxStages; ++j)
+      if (a) a[i * kMaxStages + j] = t.a[i][j];
+    if (b) b[i] = t.b[i];
+    if (c) c[i] = t.c[i];
+  }
+  return MMP_OK;
+}
+
+int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in, double* out) {
+  if (!in || !out || rows == 0) return fail(MMP_EINVAL, "bad dft arguments");
+  if (direction != -1 && direction != 1) return fail(MMP_EINVAL, "direction must be -1 or +1");
+  const int lg = ilog2_exact(n);
+  if (lg < kMinLogN || lg > kMaxLogN) return fail(MMP_ENOTSUP, "n must be a power of two in [64, 65536]");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  DeviceRes* res = nullptr;
+  int rc = ensure_device(dev, &res);
+  if (rc) return rc;
+  KernelSet ks = kernels_for(fp64 ? 1 : 0, lg);
+  const size_t bytes = (size_t)rows * n * sizeof(double2);
+  double2* d_in = nullptr;
+  double2* d_out = nullptr;
+  cudaStream_t st = nullptr;
+  CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaError_t e = cudaMalloc(&d_in, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, bytes);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_in, in, bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    DftArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = d_in;
+    a.out = d_out;
+    a.rows = (int)rows;
+    a.scale = direction < 0 ? 1.0 : 1.0 / (double)n;
+    a.tw = res->tw;
+    void* args[] = {&a};
+    e = launch(direction < 0 ? ks.dft_fwd : ks.dft_inv, dim3(rows * (unsigned)ks.C, 1, 1), ks.nthr,
+               ks.smem, ks.C, st, args);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_in);
+  cudaFree(d_out);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) return fail(MMP_ECUDA, std::string("mmp_dft: ") + cudaGetErrorString(e));
+  return MMP_OK;
+}
+
+const char* mmp_strerror(int code) {
+  switch (code) {
+    case MMP_OK: return "ok";
+    case MMP_EINVAL: return "invalid parameters";
+    case MMP_ENOMEM: return "out of memory";
+    case MMP_ECUDA: return "CUDA runtime error";
+    case MMP_ENONFINITE: return "field became non-finite";
+    case MMP_ETIMEOUT: return "timed out";
+    case MMP_ENOTSUP: return "not supported by this build";
+    case MMP_ENODEV: return "no sm_100 device";
+    case MMP_ESTATE: return "invalid state for this call";
+    default: return "unknown error";
+  }
+}
+
+const char* mmp_last_error(void) { return g_last_error.c_str(); }
+
+const char* mmp_version(void) { return "mmp_b200 0.1.0 (sm_100a)"; }
+
+uint64_t mmp_kernel_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

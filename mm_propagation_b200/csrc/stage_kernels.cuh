@@ -1,0 +1,424 @@
+// stage_kernels.cuh — the fused Lawson–RK stage kernels.
+//
+// The solver keeps the interaction-picture field in the FREQUENCY domain
+// (psi_hat = FFT(psi), FP64). The reference keeps psi in the time domain and
+// runs FFT -> *E_i -> IFFT on it in every stage
+// (src/MultimodePropagation_CPU.cpp:114-119); since the FFT is linear,
+// FFT(psi + h sum a_ij N_j) = psi_hat + h sum a_ij N_hat_j, so each stage needs
+// one inverse transform per mode to get U and one forward transform per mode
+// to turn sigma into N_hat, instead of two of each.
+//
+// One RK stage i of step n is three launches (two with Raman off):
+//   k_pair      per pair field (l<=m):  V = U_l conj(U_m) -> FFT -> * H_R -> IFFT,
+//                                       W = (1-fR) V + result          (Raman on only)
+//   k_contract  per time tile:          sigma_p = sum Q U_k W_lm        (all p)
+//   k_nu        per mode p:             FFT(sigma_p) -> N_hat_i = i sgn(gamma) conj(E_i) *.,
+//                                       [last stage: psi_hat += h sum b_j N_hat_j, monitors],
+//                                       x_hat = psi_hat + h sum a_{i+1,j} N_hat_j,
+//                                       * E_{i+1} -> IFFT -> U for the next stage
+// k_prime makes U for stage 0 when a propagate call starts. E_i = exp(i Im L_p(w) z)
+// is never stored: the phase Im L_p(w) * (z_n + c_i h) is evaluated in FP64,
+// reduced mod 2 pi in FP64 and only then passed to sincos in T.
+#pragma once
+
+#include "fft.cuh"
+
+namespace mmp {
+
+struct KParams {
+  const SolveDesc* descs;
+  TwTables tw;
+  Tableau tab;
+  int stage;
+  int pad_;
+};
+
+// Im L_p(alpha) by Horner over the per-mode polynomial (FP64).
+__device__ __forceinline__ double im_L(const double* poly, int nb, double alpha) {
+  double r = poly[nb - 1];
+  for (int j = nb - 2; j >= 0; --j) r = fma(r, alpha, poly[j]);
+  return r;
+}
+
+__device__ __forceinline__ double alpha_of(int k, int nt, double alpha_scale) {
+  // src/MultimodePropagation.cpp:167-171: index j <= nt/2 -> j, else j - nt
+  const int kk = (k <= (nt >> 1)) ? k : k - nt;
+  return alpha_scale * (double)kk;
+}
+
+// exp(i theta): theta reduced mod 2 pi in FP64 (Cody–Waite with a two-part
+// 2 pi), then sincos in precision T.
+template <typename T> __device__ __forceinline__ c2<T> expi(double theta) {
+  constexpr double kInv2Pi = 0.15915494309189533577;
+  constexpr double kTwoPiHi = 6.28318530717958623200;   // nearest double to 2 pi
+  constexpr double kTwoPiLo = 2.4492935982947063697e-16;  // 2 pi - kTwoPiHi
+  const double n = rint(theta * kInv2Pi);
+  double r = fma(-n, kTwoPiHi, theta);
+  r = fma(-n, kTwoPiLo, r);
+  if constexpr (sizeof(T) == 4) {
+    float s, c;
+    sincosf((float)r, &s, &c);
+    return make_float2(c, s);
+  } else {
+    double s, c;
+    sincos(r, &s, &c);
+    return make_double2(c, s);
+  }
+}
+
+template <typename T> __device__ __forceinline__ c2<T>* as_t2(void* p) { return reinterpret_cast<c2<T>*>(p); }
+template <typename T> __device__ __forceinline__ const c2<T>* as_t2(const void* p) { return reinterpret_cast<const c2<T>*>(p); }
+
+__device__ __forceinline__ void load_poly(double* poly, const SolveDesc& d, int p) {
+  if (threadIdx.x < d.n_beta) poly[threadIdx.x] = d.poly[p * d.n_beta + threadIdx.x];
+  __syncthreads();
+}
+
+template <typename G> __device__ __forceinline__ int cluster_rank() {
+  if constexpr (G::C == 1) return 0;
+  else return (int)cg::this_cluster().block_rank();
+}
+
+// ---- k_prime: U for stage `stage` from psi_hat (and the stored N_hat_j) -------------------
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_prime(const KParams kp) {
+  using Gm = Geo<T, LOGN>;
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* s = reinterpret_cast<V*>(smem_raw);
+  __shared__ double poly[kMaxBeta];
+  const SolveDesc& d = kp.descs[blockIdx.y];
+  const int p = blockIdx.x / Gm::C;
+  if (p >= d.M) return;  // uniform over the cluster
+  const int rank = cluster_rank<Gm>();
+  const int tid = threadIdx.x;
+  load_poly(poly, d, p);
+  const int i = kp.stage;
+  const unsigned long long n = *((volatile unsigned long long*)d.step);
+  const double zs = ((double)n + kp.tab.c[i]) * d.dz;
+  const size_t row = (size_t)p * Gm::N;
+  const size_t mstride = (size_t)d.M * Gm::N;
+  V v[Gm::E];
+#pragma unroll
+  for (int e = 0; e < Gm::E; ++e) {
+    const int k = Gm::freq_index(rank, tid, e);
+    double2 x = d.psi_hat[row + k];
+    for (int j = 0; j < i; ++j) {
+      const double aij = kp.tab.a[i][j];
+      if (aij != 0.0) {
+        const double2 nj = to_d2(as_t2<T>(d.Nh)[(size_t)j * mstride + row + k]);
+        x.x = fma(aij * d.dz, nj.x, x.x);
+        x.y = fma(aij * d.dz, nj.y, x.y);
+      }
+    }
+    const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * zs;
+    v[e] = cmul(from_d2<T>(x), expi<T>(th));
+  }
+  regs_to_time<T, LOGN>(s, v, kp.tw);
+  V* U = as_t2<T>(d.U);
+  const T inv = (T)d.inv_nt;
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    U[row + Gm::time_index(rank, u)] = cscale(s[pad(u)], inv);
+  }
+}
+
+// ---- k_pair: W_q = (1 - fR) V_q + IFFT(FFT(V_q) * H), V_q = U_l conj(U_m) ----------------
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_pair(const KParams kp) {
+  using Gm = Geo<T, LOGN>;
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* s = reinterpret_cast<V*>(smem_raw);
+  const SolveDesc& d = kp.descs[blockIdx.y];
+  const int q = blockIdx.x / Gm::C;
+  if (q >= d.P) return;
+  const int rank = cluster_rank<Gm>();
+  const int tid = threadIdx.x;
+  const int2 lm = d.pairs[q];
+  const V* U = as_t2<T>(d.U);
+  const size_t rl = (size_t)lm.x * Gm::N, rm = (size_t)lm.y * Gm::N;
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    const int t = Gm::time_index(rank, u);
+    s[pad(u)] = cmulc(U[rl + t], U[rm + t]);
+  }
+  V v[Gm::E];
+  time_to_regs<T, LOGN>(s, v, kp.tw);
+  const V* H = as_t2<T>(d.H);
+  // groups of 8 with a compiler barrier in between, so that the loads of H are
+  // not all hoisted next to the E live spectrum values (register spills)
+#pragma unroll
+  for (int g = 0; g < Gm::E; g += 8) {
+#pragma unroll
+    for (int e = g; e < g + 8 && e < Gm::E; ++e) v[e] = cmul(v[e], __ldg(&H[Gm::freq_index(rank, tid, e)]));
+    asm volatile("" ::: "memory");
+  }
+  regs_to_time<T, LOGN>(s, v, kp.tw);
+  V* W = as_t2<T>(d.W) + (size_t)q * Gm::N;
+  const T kerr = (T)d.one_minus_fR;
+  // V is formed again from U (L2-resident) rather than kept live in registers
+  // across both transforms
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    const int t = Gm::time_index(rank, u);
+    const V vt = cmulc(U[rl + t], U[rm + t]);
+    W[t] = cadd(cscale(vt, kerr), s[pad(u)]);
+  }
+}
+
+// ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) {
+  using Gm = Geo<T, LOGN>;
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* s = reinterpret_cast<V*>(smem_raw);
+  __shared__ double poly[kMaxBeta];
+  __shared__ double red[2][32];
+  const SolveDesc& d = kp.descs[blockIdx.y];
+  const int p = blockIdx.x / Gm::C;
+  if (p >= d.M) return;
+  const int rank = cluster_rank<Gm>();
+  const int tid = threadIdx.x;
+  load_poly(poly, d, p);
+  const int i = kp.stage;
+  const int S = kp.tab.s;
+  const bool last = (i == S - 1);
+  const unsigned long long n = *((volatile unsigned long long*)d.step);
+  const unsigned long long total = *((volatile unsigned long long*)d.total);
+  const double zi = ((double)n + kp.tab.c[i]) * d.dz;
+  const double znext = last ? ((double)(n + 1)) * d.dz : ((double)n + kp.tab.c[i + 1]) * d.dz;
+  const size_t row = (size_t)p * Gm::N;
+  const size_t mstride = (size_t)d.M * Gm::N;
+  const V* sig = as_t2<T>(d.sigma);
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    s[pad(u)] = sig[row + Gm::time_index(rank, u)];
+  }
+  V v[Gm::E];
+  time_to_regs<T, LOGN>(s, v, kp.tw);
+  V* Nh = as_t2<T>(d.Nh);
+  const double h = d.dz;
+  double e_part = 0.0, p_part = 0.0;
+  bool finite = true;
+#pragma unroll
+  for (int e = 0; e < Gm::E; ++e) {
+    const int k = Gm::freq_index(rank, tid, e);
+    const double alpha = alpha_of(k, Gm::N, d.alpha_scale);
+    const double L = im_L(poly, d.n_beta, alpha);
+    // N_hat_i = i sgn(gamma) conj(E_i) FFT(sigma)   (src/MultimodePropagation_CPU.cpp:231-237)
+    const V xe = cmulc(v[e], expi<T>(L * zi));
+    V nh;
+    nh.x = (T)(-d.sgn_gamma) * xe.y;
+    nh.y = (T)(d.sgn_gamma) * xe.x;
+    Nh[(size_t)i * mstride + row + k] = nh;
+    const double2 nhd = to_d2(nh);
+    double2 x = d.psi_hat[row + k];
+    if (last) {
+      // psi_{n+1} = psi_n + h sum_j b_j N_j  (src/MultimodePropagation_CPU.cpp:75-85), FP64
+      for (int j = 0; j < S; ++j) {
+        const double bj = kp.tab.b[j];
+        if (bj != 0.0) {
+          const double2 nj = (j == i) ? nhd : to_d2(Nh[(size_t)j * mstride + row + k]);
+          x.x = fma(bj * h, nj.x, x.x);
+          x.y = fma(bj * h, nj.y, x.y);
+        }
+      }
+      d.psi_hat[row + k] = x;
+      const double a2 = x.x * x.x + x.y * x.y;
+      finite = finite && isfinite(a2);
+      e_part += a2;
+      if (d.omega0_T0 != 0.0) p_part += a2 / (d.omega0_T0 + alpha);
+    } else {
+      for (int j = 0; j <= i; ++j) {
+        const double aij = kp.tab.a[i + 1][j];
+        if (aij != 0.0) {
+          const double2 nj = (j == i) ? nhd : to_d2(Nh[(size_t)j * mstride + row + k]);
+          x.x = fma(aij * h, nj.x, x.x);
+          x.y = fma(aij * h, nj.y, x.y);
+        }
+      }
+    }
+    v[e] = cmul(from_d2<T>(x), expi<T>(L * znext));
+  }
+  regs_to_time<T, LOGN>(s, v, kp.tw);
+  V* U = as_t2<T>(d.U);
+  const T inv = (T)d.inv_nt;
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    U[row + Gm::time_index(rank, u)] = cscale(s[pad(u)], inv);
+  }
+  if (last) {
+    // block reduction of the monitors, then the last CTA of this solve advances the step
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      e_part += __shfl_xor_sync(0xffffffffu, e_part, o);
+      p_part += __shfl_xor_sync(0xffffffffu, p_part, o);
+    }
+    const int finite_all = __syncthreads_and(finite ? 1 : 0);
+    if ((tid & 31) == 0) { red[0][tid >> 5] = e_part; red[1][tid >> 5] = p_part; }
+    __syncthreads();
+    if (tid == 0) {
+      double es = 0.0, ps = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { es += red[0][w]; ps += red[1][w]; }
+      if (!finite_all) atomicOr(d.status, 1);
+      if (d.monitors && total < d.mon_cap) {
+        atomicAdd(&d.energy[total], es * d.energy_scale);
+        if (d.omega0_T0 != 0.0) atomicAdd(&d.photons[total], ps * d.photon_scale);
+      }
+      __threadfence();
+      const unsigned prev = atomicAdd(d.done_ctr, 1u);
+      if (prev == (unsigned)(d.M * Gm::C) - 1u) {
+        *d.done_ctr = 0u;
+        *d.step = n + 1;
+        *d.total = total + 1;
+        __threadfence();
+      }
+    }
+  }
+}
+
+// ---- k_result: phi_p = IFFT(exp(L_p z) psi_hat_p) / conversion_factor -> io (FP64) --------
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_result(const KParams kp) {
+  using Gm = Geo<T, LOGN>;
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* s = reinterpret_cast<V*>(smem_raw);
+  __shared__ double poly[kMaxBeta];
+  const SolveDesc& d = kp.descs[blockIdx.y];
+  const int p = blockIdx.x / Gm::C;
+  if (p >= d.M) return;
+  const int rank = cluster_rank<Gm>();
+  const int tid = threadIdx.x;
+  load_poly(poly, d, p);
+  const unsigned long long n = *((volatile unsigned long long*)d.step);
+  const double z = (double)n * d.dz;
+  const size_t row = (size_t)p * Gm::N;
+  V v[Gm::E];
+#pragma unroll
+  for (int e = 0; e < Gm::E; ++e) {
+    const int k = Gm::freq_index(rank, tid, e);
+    const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * z;
+    v[e] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
+  }
+  regs_to_time<T, LOGN>(s, v, kp.tw);
+#pragma unroll 4
+  for (int e = 0; e < Gm::E; ++e) {
+    const int u = tid + e * Gm::NTHR;
+    const double2 r = to_d2(s[pad(u)]);
+    d.io[row + Gm::time_index(rank, u)] = make_double2(r.x * d.result_scale, r.y * d.result_scale);
+  }
+}
+
+// ---- k_dft: rows of FP64 samples -> transform in precision T -> rows of FP64 -------------
+// Forward (INV=false): out = scale * FFT(in). Inverse: out = scale * sum_k in[k] e^{+...}.
+struct DftArgs {
+  const double2* in;
+  double2* out;
+  int rows;
+  int pad_;
+  double scale;
+  TwTables tw;
+};
+
+template <typename T, int LOGN, bool INV>
+__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_dft(const DftArgs a) {
+  using Gm = Geo<T, LOGN>;
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* s = reinterpret_cast<V*>(smem_raw);
+  const int r = blockIdx.x / Gm::C + (int)blockIdx.y * (int)(gridDim.x / Gm::C);
+  if (r >= a.rows) return;
+  const int rank = cluster_rank<Gm>();
+  const int tid = threadIdx.x;
+  const size_t row = (size_t)r * Gm::N;
+  V v[Gm::E];
+  if constexpr (!INV) {
+#pragma unroll 4
+    for (int e = 0; e < Gm::E; ++e) {
+      const int u = tid + e * Gm::NTHR;
+      s[pad(u)] = from_d2<T>(a.in[row + Gm::time_index(rank, u)]);
+    }
+    time_to_regs<T, LOGN>(s, v, a.tw);
+#pragma unroll
+    for (int e = 0; e < Gm::E; ++e) {
+      const double2 x = to_d2(v[e]);
+      a.out[row + Gm::freq_index(rank, tid, e)] = make_double2(x.x * a.scale, x.y * a.scale);
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < Gm::E; ++e) v[e] = from_d2<T>(a.in[row + Gm::freq_index(rank, tid, e)]);
+    regs_to_time<T, LOGN>(s, v, a.tw);
+#pragma unroll 4
+    for (int e = 0; e < Gm::E; ++e) {
+      const int u = tid + e * Gm::NTHR;
+      const double2 x = to_d2(s[pad(u)]);
+      a.out[row + Gm::time_index(rank, u)] = make_double2(x.x * a.scale, x.y * a.scale);
+    }
+  }
+}
+
+// ---- k_contract: sigma_p(t) = sum_terms Q U_k(t) W(t) over a tile of t, all p ----------
+// Shared memory: U tile [M][TT] then W tile [P][TT] (Raman on). A warp covers
+// 32 consecutive t of one p, so term reads are warp-uniform and tile reads
+// are conflict-free.
+template <typename T>
+__global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT) {
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* sU = reinterpret_cast<V*>(smem_raw);
+  const SolveDesc& d = descs[blockIdx.y];
+  const int t0 = blockIdx.x * TT;
+  if (t0 >= nt) return;
+  const int M = d.M;
+  const int P = d.raman ? d.P : 0;
+  V* sW = sU + (size_t)M * TT;
+  const V* U = as_t2<T>(d.U);
+  const V* W = as_t2<T>(d.W);
+  for (int idx = threadIdx.x; idx < M * TT; idx += blockDim.x) {
+    const int m = idx / TT, tt = idx - m * TT;
+    sU[idx] = U[(size_t)m * nt + t0 + tt];
+  }
+  for (int idx = threadIdx.x; idx < P * TT; idx += blockDim.x) {
+    const int q = idx / TT, tt = idx - q * TT;
+    sW[idx] = W[(size_t)q * nt + t0 + tt];
+  }
+  __syncthreads();
+  V* sigma = as_t2<T>(d.sigma);
+  for (int idx = threadIdx.x; idx < M * TT; idx += blockDim.x) {
+    const int p = idx / TT, tt = idx - p * TT;
+    T ax = 0, ay = 0;
+    const int j1 = d.term_off[p + 1];
+    for (int j = d.term_off[p]; j < j1; ++j) {
+      const Term tm = d.terms[j];
+      V w;
+      if (d.raman) {
+        w = sW[tm.pair * TT + tt];
+        if (tm.conj) w.y = -w.y;
+      } else {
+        w = cmulc(sU[tm.l * TT + tt], sU[tm.m * TT + tt]);
+      }
+      const V uw = cmul(sU[tm.k * TT + tt], w);
+      const T qv = (T)tm.q;
+      ax = fma(qv, uw.x, ax);
+      ay = fma(qv, uw.y, ay);
+    }
+    sigma[(size_t)p * nt + t0 + tt] = mk<T>(ax, ay);
+  }
+}
+
+// FP64 rows -> T rows (used for the Raman spectrum)
+template <typename T>
+__global__ void k_to_t2(const double2* __restrict__ in, c2<T>* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = from_d2<T>(in[i]);
+}
+
+}  // namespace mmp

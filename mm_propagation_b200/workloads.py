@@ -367,7 +367,7 @@ def sweep28(seed: int = 0, index: int = 0, batch: int = 32, nt: int = 65536,
 
 def small_case(seed: int = 0, M: int = 2, nt: int = 256, n_steps: int = 20, order: int = 4,
                raman: bool = True, window: float = 10.0, fiber_length: float = 0.01,
-               peak_w: float = 2e3, nnz_target: int = 12, physical_order: bool = False,
+               peak_w: float = 200.0, nnz_target: int = 12, physical_order: bool = False,
                n_beta: int = 3, flags: int = 0) -> Problem:
     """Small seeded case for parity tests (oracle finishes in well under a second).
     GRIN-pattern coupling inserted without the pair prefix unless asked, so the

@@ -1,0 +1,161 @@
+"""GPU solver parity: libmmp_b200 through the C ABI against the reference's own
+CPU solver (golden fixtures) and the numpy restatement (live, small sizes).
+
+Tolerances (relative L2 per mode, ||phi_p - ref_p|| / ||ref_p||):
+  FP64 path (MMP_F_FP64):  1e-11  — same algorithm in FP64; differences are
+                                    rounding and transform order only.
+  FP32-bulk path:          1e-5   — FP32 transforms/contraction, FP64 phase and
+                                    field accumulation.
+"""
+import numpy as np
+import pytest
+
+import mmp_oracle as mo
+from fixtures import load, names
+from mm_propagation_b200 import capi, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-11
+TOL32 = 1e-5
+
+
+def run(mmp, prob, chunks, flags=0):
+    prob = prob.replace(flags=prob.flags | flags)
+    with mmp.Solver(prob) as s:
+        for c in chunks:
+            s.propagate(c)
+        return s.result(), s.info()
+
+
+@pytest.mark.parametrize("name", names())
+@pytest.mark.parametrize("fp64", [True, False])
+def test_golden(mmp, name, fp64):
+    prob, chunks, ref = load(name)
+    out, _ = run(mmp, prob, chunks, capi.MMP_F_FP64 if fp64 else 0)
+    err = mo.rel_l2_per_mode(out, ref).max()
+    assert err < (TOL64 if fp64 else TOL32), f"{name} fp64={fp64}: relL2 {err:.3e}"
+
+
+def test_quirk_reported(mmp):
+    prob, chunks, _ = load("grin2_quirk_raman")
+    _, info = run(mmp, prob, chunks)
+    assert info["pair_quirk_active"] == 1 and info["n_pairs"] == 4
+    prob2, chunks2, _ = load("m3_physical_order")
+    _, info2 = run(mmp, prob2, chunks2)
+    assert info2["pair_quirk_active"] == 0
+
+
+@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("raman", [True, False])
+def test_orders_live(mmp, order, raman):
+    prob = W.small_case(seed=40 + order, M=3, nt=256, n_steps=8, order=order, raman=raman)
+    ref = mo.solve(prob)
+    for fp64, tol in ((True, TOL64), (False, TOL32)):
+        out, _ = run(mmp, prob, [prob.n_steps], capi.MMP_F_FP64 if fp64 else 0)
+        assert mo.rel_l2_per_mode(out, ref).max() < tol
+
+
+def test_physical_pairs_flag(mmp):
+    prob = W.small_case(seed=51, M=3, nt=256, n_steps=10)
+    ref = mo.solve(prob, physical_pairs=True)
+    out, info = run(mmp, prob, [10], capi.MMP_F_FP64 | capi.MMP_F_PHYSICAL_PAIRS)
+    assert mo.rel_l2_per_mode(out, ref).max() < TOL64
+    assert info["pair_quirk_active"] == 0
+    # and the default reproduces the reference's slot indexing, which differs here
+    quirk = mo.solve(prob)
+    assert mo.rel_l2_per_mode(quirk, ref).max() > 1e-6
+
+
+def test_butcher7_lambda_mu(mmp):
+    prob = W.small_case(seed=52, M=2, nt=128, n_steps=6).replace(
+        rk_variant=capi.MMP_RK_BUTCHER7_LAMBDA_MU, rk_lambda=2.0, rk_mu=0.5)
+    ref = mo.solve(prob)
+    out, info = run(mmp, prob, [6], capi.MMP_F_FP64)
+    assert info["n_stages"] == 7
+    assert mo.rel_l2_per_mode(out, ref).max() < TOL64
+
+
+def test_continuous_chunks_equal_one_call(mmp):
+    # with MMP_F_CONTINUOUS, computeLawsonRK(5) + (7) is the same propagation as (12)
+    prob = W.small_case(seed=53, M=3, nt=256, n_steps=12)
+    one, _ = run(mmp, prob, [12], capi.MMP_F_FP64)
+    two, info = run(mmp, prob, [5, 7], capi.MMP_F_FP64 | capi.MMP_F_CONTINUOUS)
+    assert mo.rel_l2_per_mode(two, one).max() < 1e-13
+    assert abs(info["z"] - 12 * info["delta_z"]) < 1e-15
+    # without it, the reference's z reset makes them differ
+    reset, _ = run(mmp, prob, [5, 7], capi.MMP_F_FP64)
+    assert mo.rel_l2_per_mode(reset, one).max() > 1e-8
+
+
+def test_batch_members_match_single_solves(mmp):
+    probs = [W.small_case(seed=60 + i, M=m, nt=512, n_steps=10, nnz_target=8 + 4 * i)
+             for i, m in enumerate([2, 3, 1, 4])]
+    probs = [p.replace(flags=capi.MMP_F_FP64) for p in probs]
+    singles = [run(mmp, p, [10])[0] for p in probs]
+    with mmp.Batch(probs) as b:
+        b.propagate(10)
+        for i, p in enumerate(probs):
+            assert np.array_equal(b.result(i), singles[i]), i
+
+
+def test_set_fields_restarts(mmp):
+    prob = W.small_case(seed=70, M=2, nt=256, n_steps=10).replace(flags=capi.MMP_F_FP64)
+    other = W.small_case(seed=71, M=2, nt=256, n_steps=10)
+    with mmp.Solver(prob) as s:
+        s.propagate(10)
+        s.set_fields(other.initial_fields)
+        s.propagate(10)
+        out = s.result()
+    ref = mo.solve(prob.replace(initial_fields=other.initial_fields))
+    assert mo.rel_l2_per_mode(out, ref).max() < TOL64
+
+
+def test_noarg_propagate_uses_floor(mmp):
+    prob, chunks, ref = load("m2_noarg")
+    out, info = run(mmp, prob, chunks, capi.MMP_F_FP64)
+    assert mo.rel_l2_per_mode(out, ref).max() < TOL64
+    assert info["steps_done"] == int(np.floor(info["z_final"] / info["delta_z"]))
+
+
+def test_energy_monitor_conserved_without_raman(mmp):
+    prob = W.grin2(seed=3, nt=1024, n_steps=1000, peak_scale=0.01, raman=False)
+    with mmp.Solver(prob.replace(flags=capi.MMP_F_FP64)) as s:
+        s.propagate(200)
+        e, _ = s.monitors()
+    assert len(e) == 200
+    e0 = (np.abs(prob.initial_fields) ** 2).sum() * prob.time_window / prob.nt
+    assert abs(e[0] / e0 - 1) < 1e-6
+    assert np.abs(e / e[0] - 1).max() < 1e-6
+
+
+def test_nonfinite_is_reported(mmp):
+    # the literal reading of the four-entry pattern diverges (see workloads.grin2)
+    prob = W.grin2(seed=1, nt=256, n_steps=1000, literal=True)
+    with mmp.Solver(prob) as s:
+        with pytest.raises(mmp.MMPError) as ei:
+            s.propagate(400)
+    assert ei.value.code == capi.MMP_ENONFINITE
+
+
+@pytest.mark.parametrize("nt", [32768, 65536])
+@pytest.mark.parametrize("fp64", [True, False])
+def test_cluster_rows_live(mmp, nt, fp64):
+    # rows that span a thread-block cluster (FP32 from 2^15, FP64 from 2^14 samples)
+    prob = W.small_case(seed=80, M=2, nt=nt, n_steps=3, window=40.0, nnz_target=8)
+    ref = mo.solve(prob)
+    out, info = run(mmp, prob, [3], capi.MMP_F_FP64 if fp64 else 0)
+    assert info["cluster_ctas"] >= 2
+    assert mo.rel_l2_per_mode(out, ref).max() < (TOL64 if fp64 else TOL32)
+
+
+def test_grin6_full_rows_live(mmp):
+    # full-size rows of the 6-mode workload (M=6, NT=16384, 60 GRIN non-zeros,
+    # Raman on), 8 steps, at a power where RK4 is stable (at 5 kW the reference's
+    # own solver already loses energy within 20 steps of this step size)
+    prob = W.grin6(seed=1, n_steps=5000, peak_total_w=500.0)
+    ref = mo.solve(prob, [8])
+    a, _ = run(mmp, prob, [8])
+    b, _ = run(mmp, prob, [8], capi.MMP_F_FP64)
+    assert mo.rel_l2_per_mode(b, ref).max() < TOL64
+    assert mo.rel_l2_per_mode(a, ref).max() < TOL32
