@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=32, help="independent solves per GPU")
     ap.add_argument("--rk-per-step", type=int, default=50, help="RK steps per bench step")
     ap.add_argument("--order", type=int, default=4)
-    ap.add_argument("--peak-w", type=float, default=500.0, help="total peak power per solve (W)")
+    ap.add_argument("--peak-w", type=float, default=10.0, help="total peak power per solve (W)")
     ap.add_argument("--fp64", action="store_true", help="all-FP64 arithmetic")
     ap.add_argument("--e2e-iters", type=int, default=2)
     ap.add_argument("--cpu-steps", type=int, default=6, help="RK steps per process in the CPU sample")
