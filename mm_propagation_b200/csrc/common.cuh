@@ -51,20 +51,25 @@ template <> __device__ __forceinline__ double2 from_d2<double>(double2 a) { retu
 __host__ __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 __host__ __device__ constexpr int padded_len(int n) { return n + (n >> 5); }
 
+// SolveDesc::status bits
+constexpr int kStatusNonFinite = 1;  // the field became NaN/Inf
+constexpr int kStatusTimeout = 2;    // a bounded device-side wait gave up
+
 // Maximum number of RK stages (Butcher11) and dispersion orders handled.
 constexpr int kMaxStages = 11;
 constexpr int kMaxBeta = 13;
 
-// One contraction term of sigma_p = sum Q * U_k * W_pair (W conjugated when conj != 0).
-// For Raman-off solves (l, m) name the modes whose product U_l conj(U_m) is the pair field.
+// One contraction term of sigma_p = sum Q * U_k * W (16 bytes).
+// Raman on:  W = W_pair[a] (conjugated when conj != 0: W_ml = conj(W_lm) as h_R is real).
+// Raman off: W = U_a conj(U_b).
 struct Term {
-  int k;
-  int pair;
-  int l, m;
-  int conj;
-  int pad_;
+  unsigned short k;
+  unsigned short a;
+  unsigned short b;
+  unsigned short conj;
   double q;
 };
+static_assert(sizeof(Term) == 16, "Term layout");
 
 // Everything a kernel needs about one solve. Lives in device memory (an array
 // of these per batch); kernels index it with blockIdx.y.

@@ -140,6 +140,7 @@ template <int R, bool INV> struct RegDFT {
   }
 };
 
+
 // Twiddle tables: tw.f[L] / tw.d[L] point at 2^L entries exp(-2 pi i m / 2^L).
 struct TwTables {
   const float2* f[17];
@@ -154,7 +155,7 @@ template <typename T, int LOGN_> struct Geo {
   static constexpr int LOGN = LOGN_;
   static constexpr int N = 1 << LOGN;
   static constexpr int LOGSZ = sizeof(c2<T>) == 8 ? 3 : 4;
-  static constexpr int LOGC = (LOGN + LOGSZ > 17) ? (LOGN + LOGSZ - 17) : 0;  // <= 128 KB per CTA
+  static constexpr int LOGC = (LOGN + LOGSZ > 17) ? (LOGN + LOGSZ - 17) : 0;  // <= 128 KB of row per CTA
   static constexpr int C = 1 << LOGC;
   static constexpr int LOGL = LOGN - LOGC;
   static constexpr int NL = 1 << LOGL;
@@ -163,32 +164,60 @@ template <typename T, int LOGN_> struct Geo {
   static constexpr int LOGE = LOGE_PREF < LOGE_CAP ? LOGE_PREF : LOGE_CAP;
   static constexpr int E = 1 << LOGE;
   static constexpr int NTHR = NL / E;
-  static constexpr int CH = NL / C;  // frequencies a CTA owns per quarter-turn block
-  static constexpr int SMEM_BYTES = padded_len(NL) * (int)sizeof(c2<T>);
-  static_assert(LOGE >= LOGC, "each thread must own at least one frequency per CTA block");
+  static constexpr int LOGCH = LOGL - LOGC;
+  static constexpr int CH = NL / C;       // frequencies k a CTA combines
+  static constexpr int LOGQ = LOGL - 2;   // quarter-wave twiddle table: NL/4 entries
+  static constexpr int DATA_BYTES = padded_len(NL) * (int)sizeof(c2<T>);
+  static constexpr int TWQ_BYTES = padded_len(NL / 4) * (int)sizeof(c2<T>);
+  static constexpr int SMEM_BYTES = DATA_BYTES + TWQ_BYTES;
+  static_assert(LOGE >= LOGC, "each thread must combine at least one frequency per CTA");
   static_assert(NTHR >= 32 && NTHR <= 1024, "block size");
+  static_assert(DATA_BYTES % 16 == 0, "twiddle table alignment");
 
-  // frequency held in register slot i (0 <= i < E) of thread tid in cluster rank `rank`
-  __device__ __forceinline__ static int freq_index(int rank, int tid, int i) {
-    if constexpr (C == 1) {
-      return tid + i * NTHR;
-    } else {
-      const int jj = i >> LOGC, q = i & (C - 1);
-      return rank * CH + tid + jj * NTHR + NL * q;
-    }
+  // Spectrum layout in shared memory after a forward transform ("combined layout"):
+  // local index i holds frequency rank*CH + (i mod CH) + NL*(i div CH); for C = 1
+  // that is just i.
+  __device__ __forceinline__ static int freq_of(int rank, int i) {
+    if constexpr (C == 1) return i;
+    else return rank * CH + (i & (CH - 1)) + NL * (i >> LOGCH);
   }
-  // time of local index u
-  __device__ __forceinline__ static int time_index(int rank, int u) { return rank + C * u; }
+  // Time layout: local index u holds time rank + C*u.
+  __device__ __forceinline__ static int time_of(int rank, int u) { return rank + C * u; }
 };
 
-// One in-place Stockham pass of the local transform, then the remaining passes.
-template <typename T, int LOGL, int LOGE, bool INV, int LOGNS>
-__device__ __forceinline__ void stockham_passes(c2<T>* __restrict__ s, const c2<T>* __restrict__ tw) {
+// exp(-2 pi i m / NL) (conjugated for INV) from the quarter-wave table
+// sq[pad(m')] = exp(-2 pi i m' / NL), m' < NL/4: w(m) = (-i)^(m div NL/4) * sq[m mod NL/4].
+// The table uses the same padded index as the data: the Stockham passes read it at
+// strides of 2^a entries, which would otherwise land in one bank.
+template <typename V, bool INV, int LOGQ>
+__device__ __forceinline__ V tw_quarter(const V* __restrict__ sq, int m) {
+  const int q = m >> LOGQ;
+  const V w = sq[pad(m & ((1 << LOGQ) - 1))];
+  V r;
+  r.x = (q & 1) ? w.y : w.x;
+  r.y = (q & 1) ? -w.x : w.y;
+  if (q & 2) { r.x = -r.x; r.y = -r.y; }
+  if (INV) r.y = -r.y;
+  return r;
+}
+
+// Copy the first quarter of the size-NL table into shared memory.
+template <typename T, int LOGN>
+__device__ __forceinline__ c2<T>* load_twiddles(unsigned char* smem_raw, const TwTables& tw) {
+  using Gm = Geo<T, LOGN>;
+  c2<T>* sq = reinterpret_cast<c2<T>*>(smem_raw + Gm::DATA_BYTES);
+  const c2<T>* g = tw_table<T>(tw, Gm::LOGL);
+#pragma unroll 4
+  for (int m = threadIdx.x; m < Gm::NL / 4; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
+  return sq;
+}
+
+// One in-place Stockham pass of radix 2^LOGR at stride Ns = 2^logns (runtime).
+template <typename T, int LOGL, int LOGE, int LOGR, bool INV>
+__device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, int logns) {
   using V = c2<T>;
   constexpr int NL = 1 << LOGL, E = 1 << LOGE, NTHR = NL / E;
-  constexpr int REM = LOGL - LOGNS;
-  constexpr int LOGR = REM < LOGE ? REM : LOGE;
-  constexpr int R = 1 << LOGR, NB = E / R, Ns = 1 << LOGNS;
+  constexpr int R = 1 << LOGR, NB = E / R, LOGQ = LOGL - 2;
   const int tid = threadIdx.x;
   V v[E];
 #pragma unroll
@@ -198,50 +227,53 @@ __device__ __forceinline__ void stockham_passes(c2<T>* __restrict__ s, const c2<
     for (int r = 0; r < R; ++r) v[bf * R + r] = s[pad(j + r * (NL / R))];
   }
   __syncthreads();
+  const int nsm = (1 << logns) - 1;
 #pragma unroll
   for (int bf = 0; bf < NB; ++bf) {
     const int j = tid + bf * NTHR;
-    if constexpr (Ns > 1) {
-      const int jm = j & (Ns - 1);
+    const int jm = j & nsm;
+    if (logns > 0) {
+      const int step = jm << (LOGL - logns - LOGR);  // jm * NL / (Ns * R)
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        V w = __ldg(&tw[r * jm * (NL / (Ns * R))]);
-        if (INV) w.y = -w.y;
-        v[bf * R + r] = cmul(v[bf * R + r], w);
-      }
+      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_quarter<V, INV, LOGQ>(sq, r * step));
     }
     RegDFT<R, INV>::run(&v[bf * R]);
-    const int idxD = (j >> LOGNS) * (Ns * R) + (j & (Ns - 1));
+    const int idxD = ((j >> logns) << (logns + LOGR)) + jm;
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[pad(idxD + r * Ns)] = v[bf * R + r];
+    for (int r = 0; r < R; ++r) s[pad(idxD + (r << logns))] = v[bf * R + r];
   }
   __syncthreads();
-  if constexpr (LOGNS + LOGR < LOGL) stockham_passes<T, LOGL, LOGE, INV, LOGNS + LOGR>(s, tw);
 }
 
 // Local transform of the NL samples in shared memory (natural order in and out,
-// unnormalised). Starts with a barrier so callers may write s[] just before.
+// unnormalised). One pass body per radix keeps the instruction footprint small.
 template <typename T, int LOGN, bool INV>
-__device__ __noinline__ void local_fft_impl(c2<T>* __restrict__ s, const TwTables& tw) {
+__device__ __noinline__ void local_fft(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq) {
   using Gm = Geo<T, LOGN>;
+  constexpr int FULL = Gm::LOGL / Gm::LOGE, REM = Gm::LOGL % Gm::LOGE;
   __syncthreads();
-  stockham_passes<T, Gm::LOGL, Gm::LOGE, INV, 0>(s, tw_table<T>(tw, Gm::LOGL));
+  int logns = 0;
+#pragma unroll 1
+  for (int p = 0; p < FULL; ++p) {
+    stockham_pass<T, Gm::LOGL, Gm::LOGE, Gm::LOGE, INV>(s, sq, logns);
+    logns += Gm::LOGE;
+  }
+  if constexpr (REM > 0) stockham_pass<T, Gm::LOGL, Gm::LOGE, REM, INV>(s, sq, logns);
 }
 
-// Forward: after local_fft on every CTA of the cluster, gather this thread's E
-// frequencies into registers (slot i holds Geo::freq_index(rank, tid, i)).
+// Forward transform of the time samples in shared memory (local u = time rank + C*u);
+// leaves the spectrum in shared memory in the combined layout (Geo::freq_of).
 template <typename T, int LOGN>
-__device__ __forceinline__ void spectrum_to_regs(c2<T>* __restrict__ s, c2<T>* v, const TwTables& tw) {
+__device__ __forceinline__ void forward(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  const int tid = threadIdx.x;
-  if constexpr (Gm::C == 1) {
-#pragma unroll
-    for (int i = 0; i < Gm::E; ++i) v[i] = s[pad(tid + i * Gm::NTHR)];
-  } else {
+  local_fft<T, LOGN, false>(s, sq);
+  if constexpr (Gm::C > 1) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
+    const int tid = threadIdx.x;
     const V* twN = tw_table<T>(tw, Gm::LOGN);
+    V out[Gm::E];
     cl.sync();  // every CTA finished its local transform
 #pragma unroll
     for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
@@ -256,56 +288,60 @@ __device__ __forceinline__ void spectrum_to_regs(c2<T>* __restrict__ s, c2<T>* v
       }
       RegDFT<Gm::C, false>::run(vals);
 #pragma unroll
-      for (int q = 0; q < Gm::C; ++q) v[jj * Gm::C + q] = vals[q];
+      for (int q = 0; q < Gm::C; ++q) out[jj * Gm::C + q] = vals[q];
     }
-    cl.sync();  // all peer reads done before anyone reuses shared memory
+    cl.sync();  // all peer reads done before shared memory is overwritten
+#pragma unroll
+    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
+      const int kl = tid + jj * Gm::NTHR;
+#pragma unroll
+      for (int q = 0; q < Gm::C; ++q) s[pad(kl + Gm::CH * q)] = out[jj * Gm::C + q];
+    }
+    __syncthreads();
   }
 }
 
-// Inverse: take this thread's E frequencies from registers (same slot layout as
-// spectrum_to_regs) and leave the local inverse transforms' inputs in shared
-// memory of the right CTA; then run the local inverse transform.
+// Inverse transform of a spectrum in shared memory in the combined layout; leaves
+// the (unnormalised) time samples in shared memory, local u = time rank + C*u.
 template <typename T, int LOGN>
-__device__ __forceinline__ void regs_to_time(c2<T>* __restrict__ s, const c2<T>* v, const TwTables& tw) {
+__device__ __forceinline__ void inverse(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  const int tid = threadIdx.x;
-  if constexpr (Gm::C == 1) {
-    // each thread rewrites exactly the slots it owns; the barrier inside
-    // local_fft_impl orders these writes before the first pass reads
-#pragma unroll
-    for (int i = 0; i < Gm::E; ++i) s[pad(tid + i * Gm::NTHR)] = v[i];
-  } else {
+  if constexpr (Gm::C > 1) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
+    const int tid = threadIdx.x;
     const V* twN = tw_table<T>(tw, Gm::LOGN);
-    cl.sync();  // every CTA is running and no longer reads its shared memory
+    V out[Gm::E];
+    __syncthreads();  // the caller's writes of the spectrum are complete
 #pragma unroll
     for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
-      const int k = rank * Gm::CH + tid + jj * Gm::NTHR;
+      const int kl = tid + jj * Gm::NTHR;
+      const int k = rank * Gm::CH + kl;
       V vals[Gm::C];
 #pragma unroll
-      for (int q = 0; q < Gm::C; ++q) vals[q] = v[jj * Gm::C + q];
+      for (int q = 0; q < Gm::C; ++q) vals[q] = s[pad(kl + Gm::CH * q)];
       RegDFT<Gm::C, true>::run(vals);
 #pragma unroll
       for (int c = 0; c < Gm::C; ++c) {
         V f = vals[c];
         if (c > 0) f = cmulc(f, __ldg(&twN[c * k]));
+        out[jj * Gm::C + c] = f;
+      }
+    }
+    cl.sync();  // every CTA is running and has read its own spectrum
+#pragma unroll
+    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
+      const int k = rank * Gm::CH + tid + jj * Gm::NTHR;
+#pragma unroll
+      for (int c = 0; c < Gm::C; ++c) {
         V* peer = cl.map_shared_rank(s, c);
-        peer[pad(k)] = f;
+        peer[pad(k)] = out[jj * Gm::C + c];
       }
     }
     cl.sync();  // all peer writes landed
   }
-  local_fft_impl<T, LOGN, true>(s, tw);
-}
-
-// Forward transform of the time samples the caller left in shared memory
-// (local index u = time rank + C*u), ending with the spectrum in registers.
-template <typename T, int LOGN>
-__device__ __forceinline__ void time_to_regs(c2<T>* __restrict__ s, c2<T>* v, const TwTables& tw) {
-  local_fft_impl<T, LOGN, false>(s, tw);
-  spectrum_to_regs<T, LOGN>(s, v, tw);
+  local_fft<T, LOGN, true>(s, sq);
 }
 
 }  // namespace mmp

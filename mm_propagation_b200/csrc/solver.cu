@@ -395,13 +395,11 @@ void host_setup(const mmp_params* p, Member& s) {
         s.pairs.push_back(make_int2(lo, hi));
       }
       Term t;
-      t.k = (int)e->k;
-      t.pair = pair_idx[key];
-      t.l = le;
-      t.m = me;
-      t.conj = le > me ? 1 : 0;  // W_ml = conj(W_lm): h_R is real
-      t.pad_ = 0;
-      t.q = e->value / max_Q;  // Q_tilde (:117-136)
+      t.k = (unsigned short)e->k;
+      t.a = (unsigned short)(p->raman ? pair_idx[key] : le);
+      t.b = (unsigned short)me;
+      t.conj = (unsigned short)(le > me ? 1 : 0);  // W_ml = conj(W_lm): h_R is real
+      t.q = e->value / max_Q;                      // Q_tilde (:117-136)
       s.terms.push_back(t);
     }
   }
@@ -424,6 +422,7 @@ struct mmp_batch {
   SolveDesc* d_descs = nullptr;
   int Mmax = 0, Pmax = 0;
   int TT = 32;
+  int stage_terms = 0;
   size_t contract_smem = 0;
   KernelSet ks{}, ks64{};
   DeviceRes* dev = nullptr;
@@ -494,8 +493,8 @@ int launch_row_kernel(mmp_batch* b, const KernelSet& ks, const void* fn, int row
 
 int launch_contract(mmp_batch* b) {
   const SolveDesc* descs = b->d_descs;
-  int nt = (int)b->nt, TT = b->TT;
-  void* args[] = {(void*)&descs, &nt, &TT};
+  int nt = (int)b->nt, TT = b->TT, st = b->stage_terms;
+  void* args[] = {(void*)&descs, &nt, &TT, &st};
   dim3 grid((unsigned)(b->nt / b->TT), (unsigned)b->members.size(), 1);
   const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, b->stream, args));
@@ -549,9 +548,10 @@ int check_status(mmp_batch* b) {
     int st = 0;
     CUDA_TRY(cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
                         cudaMemcpyDeviceToHost));
-    if (st & 1) bad = 1;
+    bad |= st;
   }
-  if (bad) return fail(MMP_ENONFINITE, "the field became NaN/Inf during propagation");
+  if (bad & kStatusTimeout) return fail(MMP_ETIMEOUT, "a device-side bounded wait gave up");
+  if (bad & kStatusNonFinite) return fail(MMP_ENONFINITE, "the field became NaN/Inf during propagation");
   return MMP_OK;
 }
 
@@ -791,10 +791,15 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
     const int rows = b->Mmax + b->Pmax;
     int TT = 256;
     while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
-    while (TT > 1 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;
+    while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
     while (TT > (int)nt) TT >>= 1;
     b->TT = TT;
     b->contract_smem = (size_t)rows * TT * t2;
+    // terms follow the tiles in shared memory when they fit (else they are read through L1)
+    size_t max_terms = 0;
+    for (auto& s : b->members) max_terms = std::max(max_terms, s.terms.size());
+    b->stage_terms = b->contract_smem + max_terms * sizeof(Term) <= 200 * 1024 ? 1 : 0;
+    if (b->stage_terms) b->contract_smem += max_terms * sizeof(Term);
     e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) build_rc = fail(MMP_ECUDA, cudaGetErrorString(e));
   }

@@ -79,49 +79,51 @@ template <typename G> __device__ __forceinline__ int cluster_rank() {
   else return (int)cg::this_cluster().block_rank();
 }
 
+// Common start of a row kernel: shared memory, the quarter-wave twiddle table.
+#define MMP_ROW_SMEM()                                                 \
+  extern __shared__ __align__(16) unsigned char smem_raw[];            \
+  V* s = reinterpret_cast<V*>(smem_raw);
+
 // ---- k_prime: U for stage `stage` from psi_hat (and the stored N_hat_j) -------------------
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_prime(const KParams kp) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* s = reinterpret_cast<V*>(smem_raw);
+  MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
   const SolveDesc& d = kp.descs[blockIdx.y];
   const int p = blockIdx.x / Gm::C;
   if (p >= d.M) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
   const int i = kp.stage;
   const unsigned long long n = *((volatile unsigned long long*)d.step);
   const double zs = ((double)n + kp.tab.c[i]) * d.dz;
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
-  V v[Gm::E];
-#pragma unroll
-  for (int e = 0; e < Gm::E; ++e) {
-    const int k = Gm::freq_index(rank, tid, e);
+  const V* Nh = as_t2<T>(d.Nh);
+#pragma unroll 2
+  for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
+    const int k = Gm::freq_of(rank, li);
     double2 x = d.psi_hat[row + k];
     for (int j = 0; j < i; ++j) {
       const double aij = kp.tab.a[i][j];
       if (aij != 0.0) {
-        const double2 nj = to_d2(as_t2<T>(d.Nh)[(size_t)j * mstride + row + k]);
+        const double2 nj = to_d2(Nh[(size_t)j * mstride + row + k]);
         x.x = fma(aij * d.dz, nj.x, x.x);
         x.y = fma(aij * d.dz, nj.y, x.y);
       }
     }
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * zs;
-    v[e] = cmul(from_d2<T>(x), expi<T>(th));
+    s[pad(li)] = cmul(from_d2<T>(x), expi<T>(th));
   }
-  regs_to_time<T, LOGN>(s, v, kp.tw);
+  inverse<T, LOGN>(s, sq, kp.tw);
   V* U = as_t2<T>(d.U);
   const T inv = (T)d.inv_nt;
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
-    U[row + Gm::time_index(rank, u)] = cscale(s[pad(u)], inv);
-  }
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[row + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
 }
 
 // ---- k_pair: W_q = (1 - fR) V_q + IFFT(FFT(V_q) * H), V_q = U_l conj(U_m) ----------------
@@ -129,44 +131,33 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_pair(const KParams kp) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* s = reinterpret_cast<V*>(smem_raw);
+  MMP_ROW_SMEM();
   const SolveDesc& d = kp.descs[blockIdx.y];
   const int q = blockIdx.x / Gm::C;
   if (q >= d.P) return;
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   const int2 lm = d.pairs[q];
   const V* U = as_t2<T>(d.U);
   const size_t rl = (size_t)lm.x * Gm::N, rm = (size_t)lm.y * Gm::N;
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
-    const int t = Gm::time_index(rank, u);
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
+    const int t = Gm::time_of(rank, u);
     s[pad(u)] = cmulc(U[rl + t], U[rm + t]);
   }
-  V v[Gm::E];
-  time_to_regs<T, LOGN>(s, v, kp.tw);
+  forward<T, LOGN>(s, sq, kp.tw);
   const V* H = as_t2<T>(d.H);
-  // groups of 8 with a compiler barrier in between, so that the loads of H are
-  // not all hoisted next to the E live spectrum values (register spills)
-#pragma unroll
-  for (int g = 0; g < Gm::E; g += 8) {
-#pragma unroll
-    for (int e = g; e < g + 8 && e < Gm::E; ++e) v[e] = cmul(v[e], __ldg(&H[Gm::freq_index(rank, tid, e)]));
-    asm volatile("" ::: "memory");
-  }
-  regs_to_time<T, LOGN>(s, v, kp.tw);
+#pragma unroll 4
+  for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = cmul(s[pad(li)], __ldg(&H[Gm::freq_of(rank, li)]));
+  inverse<T, LOGN>(s, sq, kp.tw);
   V* W = as_t2<T>(d.W) + (size_t)q * Gm::N;
   const T kerr = (T)d.one_minus_fR;
-  // V is formed again from U (L2-resident) rather than kept live in registers
-  // across both transforms
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
-    const int t = Gm::time_index(rank, u);
-    const V vt = cmulc(U[rl + t], U[rm + t]);
-    W[t] = cadd(cscale(vt, kerr), s[pad(u)]);
+  // V is formed again from U (L2-resident) instead of being kept across both transforms
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
+    const int t = Gm::time_of(rank, u);
+    W[t] = cadd(cscale(cmulc(U[rl + t], U[rm + t]), kerr), s[pad(u)]);
   }
 }
 
@@ -175,8 +166,7 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* s = reinterpret_cast<V*>(smem_raw);
+  MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
   __shared__ double red[2][32];
   const SolveDesc& d = kp.descs[blockIdx.y];
@@ -184,6 +174,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
   if (p >= d.M) return;
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
   const int i = kp.stage;
   const int S = kp.tab.s;
@@ -195,24 +186,20 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
   const V* sig = as_t2<T>(d.sigma);
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
-    s[pad(u)] = sig[row + Gm::time_index(rank, u)];
-  }
-  V v[Gm::E];
-  time_to_regs<T, LOGN>(s, v, kp.tw);
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = sig[row + Gm::time_of(rank, u)];
+  forward<T, LOGN>(s, sq, kp.tw);
   V* Nh = as_t2<T>(d.Nh);
   const double h = d.dz;
   double e_part = 0.0, p_part = 0.0;
   bool finite = true;
-#pragma unroll
-  for (int e = 0; e < Gm::E; ++e) {
-    const int k = Gm::freq_index(rank, tid, e);
+#pragma unroll 2
+  for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
+    const int k = Gm::freq_of(rank, li);
     const double alpha = alpha_of(k, Gm::N, d.alpha_scale);
     const double L = im_L(poly, d.n_beta, alpha);
     // N_hat_i = i sgn(gamma) conj(E_i) FFT(sigma)   (src/MultimodePropagation_CPU.cpp:231-237)
-    const V xe = cmulc(v[e], expi<T>(L * zi));
+    const V xe = cmulc(s[pad(li)], expi<T>(L * zi));
     V nh;
     nh.x = (T)(-d.sgn_gamma) * xe.y;
     nh.y = (T)(d.sgn_gamma) * xe.x;
@@ -244,16 +231,13 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
         }
       }
     }
-    v[e] = cmul(from_d2<T>(x), expi<T>(L * znext));
+    s[pad(li)] = cmul(from_d2<T>(x), expi<T>(L * znext));
   }
-  regs_to_time<T, LOGN>(s, v, kp.tw);
+  inverse<T, LOGN>(s, sq, kp.tw);
   V* U = as_t2<T>(d.U);
   const T inv = (T)d.inv_nt;
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
-    U[row + Gm::time_index(rank, u)] = cscale(s[pad(u)], inv);
-  }
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[row + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
   if (last) {
     // block reduction of the monitors, then the last CTA of this solve advances the step
 #pragma unroll
@@ -267,7 +251,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
     if (tid == 0) {
       double es = 0.0, ps = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { es += red[0][w]; ps += red[1][w]; }
-      if (!finite_all) atomicOr(d.status, 1);
+      if (!finite_all) atomicOr(d.status, kStatusNonFinite);
       if (d.monitors && total < d.mon_cap) {
         atomicAdd(&d.energy[total], es * d.energy_scale);
         if (d.omega0_T0 != 0.0) atomicAdd(&d.photons[total], ps * d.photon_scale);
@@ -289,31 +273,29 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_result(const KParams kp) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* s = reinterpret_cast<V*>(smem_raw);
+  MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
   const SolveDesc& d = kp.descs[blockIdx.y];
   const int p = blockIdx.x / Gm::C;
   if (p >= d.M) return;
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
   const unsigned long long n = *((volatile unsigned long long*)d.step);
   const double z = (double)n * d.dz;
   const size_t row = (size_t)p * Gm::N;
-  V v[Gm::E];
-#pragma unroll
-  for (int e = 0; e < Gm::E; ++e) {
-    const int k = Gm::freq_index(rank, tid, e);
+#pragma unroll 2
+  for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
+    const int k = Gm::freq_of(rank, li);
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * z;
-    v[e] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
+    s[pad(li)] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
   }
-  regs_to_time<T, LOGN>(s, v, kp.tw);
-#pragma unroll 4
-  for (int e = 0; e < Gm::E; ++e) {
-    const int u = tid + e * Gm::NTHR;
+  inverse<T, LOGN>(s, sq, kp.tw);
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
     const double2 r = to_d2(s[pad(u)]);
-    d.io[row + Gm::time_index(rank, u)] = make_double2(r.x * d.result_scale, r.y * d.result_scale);
+    d.io[row + Gm::time_of(rank, u)] = make_double2(r.x * d.result_scale, r.y * d.result_scale);
   }
 }
 
@@ -332,78 +314,131 @@ template <typename T, int LOGN, bool INV>
 __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_dft(const DftArgs a) {
   using Gm = Geo<T, LOGN>;
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* s = reinterpret_cast<V*>(smem_raw);
-  const int r = blockIdx.x / Gm::C + (int)blockIdx.y * (int)(gridDim.x / Gm::C);
+  MMP_ROW_SMEM();
+  const int r = blockIdx.x / Gm::C;
   if (r >= a.rows) return;
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  const V* sq = load_twiddles<T, LOGN>(smem_raw, a.tw);
   const size_t row = (size_t)r * Gm::N;
-  V v[Gm::E];
   if constexpr (!INV) {
-#pragma unroll 4
-    for (int e = 0; e < Gm::E; ++e) {
-      const int u = tid + e * Gm::NTHR;
-      s[pad(u)] = from_d2<T>(a.in[row + Gm::time_index(rank, u)]);
-    }
-    time_to_regs<T, LOGN>(s, v, a.tw);
-#pragma unroll
-    for (int e = 0; e < Gm::E; ++e) {
-      const double2 x = to_d2(v[e]);
-      a.out[row + Gm::freq_index(rank, tid, e)] = make_double2(x.x * a.scale, x.y * a.scale);
+#pragma unroll 8
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = from_d2<T>(a.in[row + Gm::time_of(rank, u)]);
+    forward<T, LOGN>(s, sq, a.tw);
+#pragma unroll 8
+    for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
+      const double2 x = to_d2(s[pad(li)]);
+      a.out[row + Gm::freq_of(rank, li)] = make_double2(x.x * a.scale, x.y * a.scale);
     }
   } else {
-#pragma unroll
-    for (int e = 0; e < Gm::E; ++e) v[e] = from_d2<T>(a.in[row + Gm::freq_index(rank, tid, e)]);
-    regs_to_time<T, LOGN>(s, v, a.tw);
-#pragma unroll 4
-    for (int e = 0; e < Gm::E; ++e) {
-      const int u = tid + e * Gm::NTHR;
+#pragma unroll 8
+    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = from_d2<T>(a.in[row + Gm::freq_of(rank, li)]);
+    inverse<T, LOGN>(s, sq, a.tw);
+#pragma unroll 8
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
       const double2 x = to_d2(s[pad(u)]);
-      a.out[row + Gm::time_index(rank, u)] = make_double2(x.x * a.scale, x.y * a.scale);
+      a.out[row + Gm::time_of(rank, u)] = make_double2(x.x * a.scale, x.y * a.scale);
     }
   }
 }
 
+// ---- bulk-async copies (TMA engine) into shared memory, completing on an mbarrier -------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// global -> this CTA's shared memory; dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Wait for phase `parity` of the mbarrier, giving up after `max_iter` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned max_iter) {
+  const unsigned a = smem_addr(bar);
+  for (unsigned it = 0; it < max_iter; ++it) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+constexpr unsigned kMaxWaitPolls = 1u << 24;  // far above any copy time; then report, not hang
+
 // ---- k_contract: sigma_p(t) = sum_terms Q U_k(t) W(t) over a tile of t, all p ----------
-// Shared memory: U tile [M][TT] then W tile [P][TT] (Raman on). A warp covers
-// 32 consecutive t of one p, so term reads are warp-uniform and tile reads
-// are conflict-free.
+// The U tile [M][TT] and the W tile [P][TT] (Raman on) arrive in shared memory as
+// one bulk-async copy per row segment (TT contiguous samples), issued by the
+// threads of the CTA and counted on one mbarrier. A warp then covers 32
+// consecutive t of one p, so term reads are warp-uniform and tile reads are
+// conflict-free.
 template <typename T>
-__global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT) {
+__global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
+                                                  int stage_terms) {
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long bar;
   V* sU = reinterpret_cast<V*>(smem_raw);
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TT;
   if (t0 >= nt) return;
   const int M = d.M;
-  const int P = d.raman ? d.P : 0;
+  const int raman = d.raman;
+  const int P = raman ? d.P : 0;
   V* sW = sU + (size_t)M * TT;
+  const int n_terms = d.term_off[M];
+  const Term* terms = d.terms;
+  if (stage_terms) {
+    Term* st = reinterpret_cast<Term*>(sU + (size_t)(M + P) * TT);
+    for (int j = threadIdx.x; j < n_terms; j += blockDim.x) st[j] = d.terms[j];
+    terms = st;
+  }
   const V* U = as_t2<T>(d.U);
   const V* W = as_t2<T>(d.W);
-  for (int idx = threadIdx.x; idx < M * TT; idx += blockDim.x) {
-    const int m = idx / TT, tt = idx - m * TT;
-    sU[idx] = U[(size_t)m * nt + t0 + tt];
-  }
-  for (int idx = threadIdx.x; idx < P * TT; idx += blockDim.x) {
-    const int q = idx / TT, tt = idx - q * TT;
-    sW[idx] = W[(size_t)q * nt + t0 + tt];
+  const unsigned row_bytes = (unsigned)(TT * sizeof(V));
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, (unsigned)(M + P) * row_bytes);
   }
   __syncthreads();
+  for (int r = threadIdx.x; r < M + P; r += blockDim.x) {
+    const V* src = (r < M) ? U + (size_t)r * nt + t0 : W + (size_t)(r - M) * nt + t0;
+    bulk_g2s(sU + (size_t)r * TT, src, row_bytes, &bar);
+  }
+  // every thread polls with a bound; the barrier makes the outcome CTA-uniform and
+  // also publishes the staged terms
+  const bool landed = mbar_wait(&bar, 0, kMaxWaitPolls);
+  if (!__syncthreads_and(landed ? 1 : 0)) {
+    if (threadIdx.x == 0) atomicOr(d.status, kStatusTimeout);
+    // give the copies a second bounded chance to land before the CTA leaves
+    mbar_wait(&bar, 0, kMaxWaitPolls);
+    return;
+  }
   V* sigma = as_t2<T>(d.sigma);
   for (int idx = threadIdx.x; idx < M * TT; idx += blockDim.x) {
     const int p = idx / TT, tt = idx - p * TT;
     T ax = 0, ay = 0;
     const int j1 = d.term_off[p + 1];
     for (int j = d.term_off[p]; j < j1; ++j) {
-      const Term tm = d.terms[j];
+      const Term tm = terms[j];
       V w;
-      if (d.raman) {
-        w = sW[tm.pair * TT + tt];
+      if (raman) {
+        w = sW[tm.a * TT + tt];
         if (tm.conj) w.y = -w.y;
       } else {
-        w = cmulc(sU[tm.l * TT + tt], sU[tm.m * TT + tt]);
+        w = cmulc(sU[tm.a * TT + tt], sU[tm.b * TT + tt]);
       }
       const V uw = cmul(sU[tm.k * TT + tt], w);
       const T qv = (T)tm.q;
