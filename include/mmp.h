@@ -196,6 +196,21 @@ int mmp_tableau(uint32_t method_order, int32_t rk_variant, double rk_lambda, dou
  * by 1/n, as the reference's Inverse_DFT. fp64 = 0 transforms in FP32, 1 in FP64. */
 int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in, double* out);
 
+/* No counterpart in the reference. The same transform as mmp_dft (same arguments,
+ * same results) for callers that must not allocate device memory when they call it:
+ * a host whose device memory pool belongs to its own caching allocator, a loop that
+ * cannot take the device synchronisation a cudaMalloc/cudaFree pair may cause, or a
+ * plugin with a memory budget fixed at load time. mmp_dft allocates device copies of
+ * in/out on every call; this one stages them in a static device array of about
+ * 19 MiB (twiddle tables plus room for 2^20 complex FP64 samples) that every GPU
+ * loading the library holds until exit, and calls no cudaMalloc or cudaFree.
+ * rows * n above 2^20 returns MMP_EINVAL. The first call on a device (with it
+ * current) looks up the array's device address and fills the twiddle tables with a
+ * kernel launch: make that first call before any stream capture. All calls on a
+ * device share the staging buffer, which keeps the last call's data; calls that
+ * overlap on the GPU race, so serialise calls from several host threads. */
+int mmp_dft_noalloc(uint32_t n, uint32_t rows, int direction, int fp64, const double* in, double* out);
+
 /* ---- library facts ----------------------------------------------------------------- */
 const char* mmp_strerror(int code);
 /* Text of the last failure on the calling thread (empty when none). */

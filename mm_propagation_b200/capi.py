@@ -108,6 +108,8 @@ SIGNATURES = {
                               C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mmp_dft": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
                          C.POINTER(C.c_double)]),
+    "mmp_dft_noalloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]),
     "mmp_strerror": (C.c_char_p, [C.c_int]),
     "mmp_last_error": (C.c_char_p, []),
     "mmp_version": (C.c_char_p, []),
