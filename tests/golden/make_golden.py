@@ -66,7 +66,31 @@ def save(name, prob, chunks, phi, seconds):
                                                                    "raman", "n_nonzeros")}}
 
 
+def dropin_golden():
+    """Build tests/dropin/two_mode_driver.cpp against the reference's own headers and
+    CPU objects (oracle/_ref, from `make -C oracle`), run it, store its output."""
+    import subprocess
+    import tempfile
+    ref_dir = os.environ.get("REF_DIR", "/root/reference")
+    objs = sorted(os.path.join(ROOT, "oracle", "_ref", f) for f in os.listdir(os.path.join(ROOT, "oracle", "_ref"))
+                  if f.startswith("ref_") and f.endswith(".o") and f != "ref_driver.o")
+    objs.append(os.path.join(ROOT, "oracle", "_ref", "fftw3_shim.o"))
+    with tempfile.TemporaryDirectory() as td:
+        exe = os.path.join(td, "drv_ref")
+        subprocess.run(["/usr/bin/g++", "-O3", "-std=c++11", "-fopenmp", "-DMMP_REFERENCE_BUILD",
+                        "-I" + os.path.join(ref_dir, "include"), "-I" + os.path.join(ROOT, "oracle", "fftw_shim"),
+                        os.path.join(ROOT, "tests", "dropin", "two_mode_driver.cpp"), *objs, "-o", exe], check=True)
+        out = os.path.join(td, "out.txt")
+        subprocess.run([exe, out], check=True)
+        a = np.loadtxt(out)
+    phi = (a[:, 0] + 1j * a[:, 1]).reshape(2, -1)
+    assert np.isfinite(phi).all()
+    np.savez_compressed(os.path.join(HERE, "dropin_two_mode.npz"), result=phi)
+    print(f"dropin_two_mode: |phi|max {np.abs(phi).max():.3e}")
+
+
 def main():
+    dropin_golden()
     manifest = []
     for name, (prob, chunks) in cases().items():
         phi, sec = ref_lib.run(prob, chunks)
