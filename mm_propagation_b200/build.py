@@ -28,6 +28,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE] + ARCH
 LOGN_RANGE = range(6, 17)
+# row-split variants (kernel_table.h kSplit*): log2 NT ranges per precision
+SPLIT_F32 = range(12, 16)
+SPLIT_F64 = range(11, 15)
 
 
 def nvcc() -> str:
@@ -52,10 +55,12 @@ def _stale(target: str, deps) -> bool:
 def _units():
     units = []
     inst = os.path.join(CSRC, "kern_inst.cu")
-    for tag, real in (("f32", "float"), ("f64", "double")):
+    for tag, real, split in (("f32", "float", SPLIT_F32), ("f64", "double", SPLIT_F64)):
         for L in LOGN_RANGE:
-            obj = os.path.join(BUILD, f"kern_{tag}_{L}.o")
-            units.append((inst, obj, [f"-DMMP_REAL={real}", f"-DMMP_LOGN={L}", f"-DMMP_TAG={tag}"]))
+            for xc in ((0, 1) if L in split else (0,)):
+                obj = os.path.join(BUILD, f"kern_{tag}_{L}_x{xc}.o")
+                units.append((inst, obj, [f"-DMMP_REAL={real}", f"-DMMP_LOGN={L}", f"-DMMP_TAG={tag}",
+                                          f"-DMMP_XC={xc}"]))
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         if os.path.basename(src) == "kern_inst.cu":
             continue

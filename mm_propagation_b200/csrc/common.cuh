@@ -59,14 +59,17 @@ constexpr int kStatusTimeout = 2;    // a bounded device-side wait gave up
 constexpr int kMaxStages = 11;
 constexpr int kMaxBeta = 13;
 
-// One contraction term of sigma_p = sum Q * U_k * W (16 bytes).
-// Raman on:  W = W_pair[a] (conjugated when conj != 0: W_ml = conj(W_lm) as h_R is real).
-// Raman off: W = U_a conj(U_b).
+// One contraction term of sigma_p = sum Q * U_k * W (16 bytes), with
+//   Raman off: W = U_l conj(U_m)
+//   Raman on:  W = (1 - fR) U_l conj(U_m) + R_pair, R_pair the Raman convolution of the
+//              pair field l<=m; for l > m the stored pair is (m, l) and R is conjugated
+//              (R_lm = conj(R_ml) because h_R is real).
+// pc = pair index | (conj << 15).
 struct Term {
   unsigned short k;
-  unsigned short a;
-  unsigned short b;
-  unsigned short conj;
+  unsigned short l;
+  unsigned short m;
+  unsigned short pc;
   double q;
 };
 static_assert(sizeof(Term) == 16, "Term layout");
@@ -77,7 +80,7 @@ struct SolveDesc {
   int M;            // modes
   int P;            // distinct pair fields (l <= m) formed on the device
   int n_beta;       // polynomial coefficients per mode
-  int raman;        // 1: W = (1-fR) V + h_R (*) V; 0: W = V
+  int raman;        // 1: Raman on (contraction adds R = h_R (*) V to (1-fR) V)
   double alpha_scale;   // 2*pi / t_final
   double dz;            // h (dimensionless)
   double sgn_gamma;     // +1 / -1
@@ -91,7 +94,7 @@ struct SolveDesc {
   double2* psi_hat;     // [M][NT] interaction-picture field, frequency domain, FP64
   void* Nh;             // [s][M][NT] stage derivatives, frequency domain (T2)
   void* U;              // [M][NT] stage field, time domain (T2)
-  void* W;              // [P][NT] pair fields, time domain (T2)
+  void* W;              // [P][NT] Raman-convolved pair fields R, time domain (T2)
   void* sigma;          // [M][NT] contraction output, time domain (T2)
   const void* H;        // [NT] scaled Raman spectrum (T2) or null
   double2* io;          // [M][NT] FP64 staging for upload / result

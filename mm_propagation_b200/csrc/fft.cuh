@@ -151,11 +151,11 @@ template <> __device__ __forceinline__ const float2* tw_table<float>(const TwTab
 template <> __device__ __forceinline__ const double2* tw_table<double>(const TwTables& t, int L) { return t.d[L]; }
 
 // Geometry of one row transform.
-template <typename T, int LOGN_> struct Geo {
+template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   static constexpr int LOGN = LOGN_;
   static constexpr int N = 1 << LOGN;
   static constexpr int LOGSZ = sizeof(c2<T>) == 8 ? 3 : 4;
-  static constexpr int LOGC = (LOGN + LOGSZ > 17) ? (LOGN + LOGSZ - 17) : 0;  // <= 128 KB of row per CTA
+  static constexpr int LOGC = ((LOGN + LOGSZ > 17) ? (LOGN + LOGSZ - 17) : 0) + XC_;  // <= 128 KB of row per CTA, times 2^XC_ CTAs
   static constexpr int C = 1 << LOGC;
   static constexpr int LOGL = LOGN - LOGC;
   static constexpr int NL = 1 << LOGL;
@@ -170,6 +170,8 @@ template <typename T, int LOGN_> struct Geo {
   static constexpr int DATA_BYTES = padded_len(NL) * (int)sizeof(c2<T>);
   static constexpr int TWQ_BYTES = padded_len(NL / 4) * (int)sizeof(c2<T>);
   static constexpr int SMEM_BYTES = DATA_BYTES + TWQ_BYTES;
+  // split rows (XC_ > 0) are sized so that two CTAs share an SM
+  static constexpr int MIN_BLOCKS = (XC_ > 0 && SMEM_BYTES <= 110 * 1024 && NTHR <= 512) ? 2 : 1;
   static_assert(LOGE >= LOGC, "each thread must combine at least one frequency per CTA");
   static_assert(NTHR >= 32 && NTHR <= 1024, "block size");
   static_assert(DATA_BYTES % 16 == 0, "twiddle table alignment");
@@ -202,9 +204,9 @@ __device__ __forceinline__ V tw_quarter(const V* __restrict__ sq, int m) {
 }
 
 // Copy the first quarter of the size-NL table into shared memory.
-template <typename T, int LOGN>
+template <typename T, int LOGN, int XC>
 __device__ __forceinline__ c2<T>* load_twiddles(unsigned char* smem_raw, const TwTables& tw) {
-  using Gm = Geo<T, LOGN>;
+  using Gm = Geo<T, LOGN, XC>;
   c2<T>* sq = reinterpret_cast<c2<T>*>(smem_raw + Gm::DATA_BYTES);
   const c2<T>* g = tw_table<T>(tw, Gm::LOGL);
 #pragma unroll 4
@@ -247,9 +249,9 @@ __device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ s, const c2<T>
 
 // Local transform of the NL samples in shared memory (natural order in and out,
 // unnormalised). One pass body per radix keeps the instruction footprint small.
-template <typename T, int LOGN, bool INV>
+template <typename T, int LOGN, int XC, bool INV>
 __device__ __noinline__ void local_fft(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq) {
-  using Gm = Geo<T, LOGN>;
+  using Gm = Geo<T, LOGN, XC>;
   constexpr int FULL = Gm::LOGL / Gm::LOGE, REM = Gm::LOGL % Gm::LOGE;
   __syncthreads();
   int logns = 0;
@@ -263,11 +265,11 @@ __device__ __noinline__ void local_fft(c2<T>* __restrict__ s, const c2<T>* __res
 
 // Forward transform of the time samples in shared memory (local u = time rank + C*u);
 // leaves the spectrum in shared memory in the combined layout (Geo::freq_of).
-template <typename T, int LOGN>
+template <typename T, int LOGN, int XC>
 __device__ __forceinline__ void forward(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
-  using Gm = Geo<T, LOGN>;
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
-  local_fft<T, LOGN, false>(s, sq);
+  local_fft<T, LOGN, XC, false>(s, sq);
   if constexpr (Gm::C > 1) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
@@ -303,9 +305,9 @@ __device__ __forceinline__ void forward(c2<T>* __restrict__ s, const c2<T>* __re
 
 // Inverse transform of a spectrum in shared memory in the combined layout; leaves
 // the (unnormalised) time samples in shared memory, local u = time rank + C*u.
-template <typename T, int LOGN>
+template <typename T, int LOGN, int XC>
 __device__ __forceinline__ void inverse(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
-  using Gm = Geo<T, LOGN>;
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   if constexpr (Gm::C > 1) {
     cg::cluster_group cl = cg::this_cluster();
@@ -341,7 +343,7 @@ __device__ __forceinline__ void inverse(c2<T>* __restrict__ s, const c2<T>* __re
     }
     cl.sync();  // all peer writes landed
   }
-  local_fft<T, LOGN, true>(s, sq);
+  local_fft<T, LOGN, XC, true>(s, sq);
 }
 
 }  // namespace mmp

@@ -1,30 +1,39 @@
-// kern_inst.cu — compiled once per (precision, log2 NT) with
-//   -DMMP_REAL=float|double -DMMP_LOGN=<6..16> -DMMP_TAG=f32|f64
-// so that the heavily unrolled FFT kernels build in parallel.
+// kern_inst.cu — compiled once per (precision, log2 NT, row split) with
+//   -DMMP_REAL=float|double -DMMP_LOGN=<6..16> -DMMP_TAG=f32|f64 -DMMP_XC=<0|1>
+// so that the heavily unrolled FFT kernels build in parallel. MMP_XC = 1 splits
+// every row over twice as many CTAs (a cluster), halving each CTA's shared memory
+// and registers so that two CTAs share an SM; the solver times both and keeps the
+// faster (see solver.cu, autotune).
 #include "kernel_table.h"
 #include "stage_kernels.cuh"
 
-#define MMP_CAT3_(a, b, c) a##b##_##c
-#define MMP_CAT3(a, b, c) MMP_CAT3_(a, b, c)
+#ifndef MMP_XC
+#define MMP_XC 0
+#endif
+
+#define MMP_CAT4_(a, b, c, d) a##b##_##c##_##d
+#define MMP_CAT4(a, b, c, d) MMP_CAT4_(a, b, c, d)
 
 namespace mmp {
 
-KernelSet MMP_CAT3(make_kernels_, MMP_TAG, MMP_LOGN)() {
+KernelSet MMP_CAT4(make_kernels_, MMP_TAG, MMP_LOGN, MMP_XC)() {
   using T = MMP_REAL;
   constexpr int L = MMP_LOGN;
-  using Gm = Geo<T, L>;
+  constexpr int X = MMP_XC;
+  using Gm = Geo<T, L, X>;
   KernelSet k;
-  k.prime = (const void*)&k_prime<T, L>;
-  k.pair = (const void*)&k_pair<T, L>;
-  k.nu = (const void*)&k_nu<T, L>;
-  k.result = (const void*)&k_result<T, L>;
-  k.dft_fwd = (const void*)&k_dft<T, L, false>;
-  k.dft_inv = (const void*)&k_dft<T, L, true>;
+  k.prime = (const void*)&k_prime<T, L, X>;
+  k.pair = (const void*)&k_pair<T, L, X>;
+  k.nu = (const void*)&k_nu<T, L, X>;
+  k.result = (const void*)&k_result<T, L, X>;
+  k.dft_fwd = (const void*)&k_dft<T, L, X, false>;
+  k.dft_inv = (const void*)&k_dft<T, L, X, true>;
   k.C = Gm::C;
   k.nthr = Gm::NTHR;
   k.smem = Gm::SMEM_BYTES;
   k.logn = L;
   k.fp64 = sizeof(T) == 8;
+  k.xc = X;
   return k;
 }
 

@@ -16,12 +16,17 @@ struct KernelSet {
   int smem = 0;   // dynamic shared memory per CTA, bytes
   int logn = 0;
   int fp64 = 0;
+  int xc = 0;     // rows split over 2^xc times the minimal number of CTAs
 };
 
 constexpr int kMinLogN = 6;
 constexpr int kMaxLogN = 16;
 
-// Defined in the kern_inst.cu objects; returns an empty set for sizes not built.
-KernelSet kernels_for(int fp64, int logn);
+// Row-split variants built besides xc = 0 (FP32 / FP64 ranges of log2 NT).
+constexpr int kSplitMinLogN32 = 12, kSplitMaxLogN32 = 15;
+constexpr int kSplitMinLogN64 = 11, kSplitMaxLogN64 = 14;
+
+// Defined in the kern_inst.cu objects; returns an empty set for variants not built.
+KernelSet kernels_for(int fp64, int logn, int xc = 0);
 
 }  // namespace mmp

@@ -8,6 +8,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -22,29 +23,44 @@ using namespace mmp;
 
 // ---------------------------------------------------------------------------------------
 // instantiated kernel sets (kern_inst.cu objects)
-#define MMP_DECL(tag, L) KernelSet make_kernels_##tag##_##L();
+#define MMP_DECL(tag, L, X) KernelSet make_kernels_##tag##_##L##_##X();
 #define MMP_DECL_ALL(tag) \
-  MMP_DECL(tag, 6) MMP_DECL(tag, 7) MMP_DECL(tag, 8) MMP_DECL(tag, 9) MMP_DECL(tag, 10) \
-  MMP_DECL(tag, 11) MMP_DECL(tag, 12) MMP_DECL(tag, 13) MMP_DECL(tag, 14) MMP_DECL(tag, 15) \
-  MMP_DECL(tag, 16)
+  MMP_DECL(tag, 6, 0) MMP_DECL(tag, 7, 0) MMP_DECL(tag, 8, 0) MMP_DECL(tag, 9, 0) MMP_DECL(tag, 10, 0) \
+  MMP_DECL(tag, 11, 0) MMP_DECL(tag, 12, 0) MMP_DECL(tag, 13, 0) MMP_DECL(tag, 14, 0) MMP_DECL(tag, 15, 0) \
+  MMP_DECL(tag, 16, 0)
 namespace mmp {
 MMP_DECL_ALL(f32)
 MMP_DECL_ALL(f64)
+MMP_DECL(f32, 12, 1) MMP_DECL(f32, 13, 1) MMP_DECL(f32, 14, 1) MMP_DECL(f32, 15, 1)
+MMP_DECL(f64, 11, 1) MMP_DECL(f64, 12, 1) MMP_DECL(f64, 13, 1) MMP_DECL(f64, 14, 1)
 
-KernelSet kernels_for(int fp64, int logn) {
-#define MMP_CASE(tag, L) case L: return make_kernels_##tag##_##L();
+KernelSet kernels_for(int fp64, int logn, int xc) {
+#define MMP_CASE(tag, L, X) case L: return make_kernels_##tag##_##L##_##X();
+  if (xc == 1) {
+    if (fp64) {
+      switch (logn) {
+        MMP_CASE(f64, 11, 1) MMP_CASE(f64, 12, 1) MMP_CASE(f64, 13, 1) MMP_CASE(f64, 14, 1)
+        default: return KernelSet();
+      }
+    }
+    switch (logn) {
+      MMP_CASE(f32, 12, 1) MMP_CASE(f32, 13, 1) MMP_CASE(f32, 14, 1) MMP_CASE(f32, 15, 1)
+      default: return KernelSet();
+    }
+  }
+  if (xc != 0) return KernelSet();
   if (fp64) {
     switch (logn) {
-      MMP_CASE(f64, 6) MMP_CASE(f64, 7) MMP_CASE(f64, 8) MMP_CASE(f64, 9) MMP_CASE(f64, 10)
-      MMP_CASE(f64, 11) MMP_CASE(f64, 12) MMP_CASE(f64, 13) MMP_CASE(f64, 14) MMP_CASE(f64, 15)
-      MMP_CASE(f64, 16)
+      MMP_CASE(f64, 6, 0) MMP_CASE(f64, 7, 0) MMP_CASE(f64, 8, 0) MMP_CASE(f64, 9, 0) MMP_CASE(f64, 10, 0)
+      MMP_CASE(f64, 11, 0) MMP_CASE(f64, 12, 0) MMP_CASE(f64, 13, 0) MMP_CASE(f64, 14, 0) MMP_CASE(f64, 15, 0)
+      MMP_CASE(f64, 16, 0)
       default: return KernelSet();
     }
   }
   switch (logn) {
-    MMP_CASE(f32, 6) MMP_CASE(f32, 7) MMP_CASE(f32, 8) MMP_CASE(f32, 9) MMP_CASE(f32, 10)
-    MMP_CASE(f32, 11) MMP_CASE(f32, 12) MMP_CASE(f32, 13) MMP_CASE(f32, 14) MMP_CASE(f32, 15)
-    MMP_CASE(f32, 16)
+    MMP_CASE(f32, 6, 0) MMP_CASE(f32, 7, 0) MMP_CASE(f32, 8, 0) MMP_CASE(f32, 9, 0) MMP_CASE(f32, 10, 0)
+    MMP_CASE(f32, 11, 0) MMP_CASE(f32, 12, 0) MMP_CASE(f32, 13, 0) MMP_CASE(f32, 14, 0) MMP_CASE(f32, 15, 0)
+    MMP_CASE(f32, 16, 0)
     default: return KernelSet();
   }
 #undef MMP_CASE
@@ -117,13 +133,14 @@ int ensure_device(int dev, DeviceRes** out) {
   r.tw_mem = mem;
   // dynamic shared memory opt-in for every instantiated kernel
   for (int fp64 = 0; fp64 < 2; ++fp64)
-    for (int L = kMinLogN; L <= kMaxLogN; ++L) {
-      KernelSet ks = kernels_for(fp64, L);
-      if (!ks.prime) continue;
-      const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.result, ks.dft_fwd, ks.dft_inv};
-      for (const void* f : fns)
-        CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
-    }
+    for (int L = kMinLogN; L <= kMaxLogN; ++L)
+      for (int xc = 0; xc < 2; ++xc) {
+        KernelSet ks = kernels_for(fp64, L, xc);
+        if (!ks.prime) continue;
+        const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.result, ks.dft_fwd, ks.dft_inv};
+        for (const void* f : fns)
+          CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+      }
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<double>,
@@ -396,10 +413,10 @@ void host_setup(const mmp_params* p, Member& s) {
       }
       Term t;
       t.k = (unsigned short)e->k;
-      t.a = (unsigned short)(p->raman ? pair_idx[key] : le);
-      t.b = (unsigned short)me;
-      t.conj = (unsigned short)(le > me ? 1 : 0);  // W_ml = conj(W_lm): h_R is real
-      t.q = e->value / max_Q;                      // Q_tilde (:117-136)
+      t.l = (unsigned short)le;
+      t.m = (unsigned short)me;
+      t.pc = (unsigned short)(pair_idx[key] | (le > me ? 0x8000 : 0));  // R_ml = conj(R_lm): h_R is real
+      t.q = e->value / max_Q;                                           // Q_tilde (:117-136)
       s.terms.push_back(t);
     }
   }
@@ -498,6 +515,66 @@ int launch_contract(mmp_batch* b) {
   dim3 grid((unsigned)(b->nt / b->TT), (unsigned)b->members.size(), 1);
   const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, b->stream, args));
+  return MMP_OK;
+}
+
+// ---- autotuner: rows on one CTA (or the minimal cluster) vs split over twice as many
+// CTAs. Both variants' pair and per-mode kernels are timed on this batch's own buffers
+// at stage 0 (which rewrites only W, U and N_hat_0: all of them are recomputed before
+// they are read again), and the faster set is kept. Decisions are cached per shape.
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_tune_cache;
+
+int time_variant(mmp_batch* b, const KernelSet& ks, float* ms) {
+  const int nsol = (int)b->members.size();
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int rc = MMP_OK;
+  for (int rep = 0; rep < 4 && rc == MMP_OK; ++rep) {  // rep 0 warms up
+    if (rep == 1) cudaEventRecord(e0, b->stream);
+    if (b->raman && b->Pmax > 0) rc = launch_row_kernel(b, ks, ks.pair, b->Pmax, nsol, 0, b->d_descs);
+    if (rc == MMP_OK) rc = launch_row_kernel(b, ks, ks.nu, b->Mmax, nsol, 0, b->d_descs);
+  }
+  cudaEventRecord(e1, b->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float f = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(MMP_ECUDA, cudaGetErrorString(e));
+  *ms = f;
+  return MMP_OK;
+}
+
+int autotune(mmp_batch* b) {
+  const KernelSet alt = kernels_for(b->fp64 ? 1 : 0, b->logn, 1);
+  if (!alt.prime) return MMP_OK;
+  if (const char* env = std::getenv("MMP_ROW_SPLIT")) {  // 0 / 1 forces a variant
+    if (std::atoi(env) == 1) b->ks = alt;
+    return MMP_OK;
+  }
+  const std::vector<int> key = {b->device, b->fp64 ? 1 : 0, b->logn, b->Mmax, b->Pmax,
+                                (int)b->members.size(), b->raman ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      if (it->second == 1) b->ks = alt;
+      return MMP_OK;
+    }
+  }
+  const uint64_t counted = g_launches.load();
+  float t0 = 0.f, t1 = 0.f;
+  int rc = time_variant(b, b->ks, &t0);
+  if (rc == MMP_OK) rc = time_variant(b, alt, &t1);
+  g_launches.store(counted);  // tuning launches are not solver work
+  if (rc) return rc;
+  const int pick = (t1 < t0) ? 1 : 0;
+  if (pick) b->ks = alt;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = pick;
   return MMP_OK;
 }
 
@@ -800,6 +877,7 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
     for (auto& s : b->members) max_terms = std::max(max_terms, s.terms.size());
     b->stage_terms = b->contract_smem + max_terms * sizeof(Term) <= 200 * 1024 ? 1 : 0;
     if (b->stage_terms) b->contract_smem += max_terms * sizeof(Term);
+    build_rc = autotune(b);
     e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) build_rc = fail(MMP_ECUDA, cudaGetErrorString(e));
   }

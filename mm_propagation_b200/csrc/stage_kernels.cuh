@@ -9,9 +9,10 @@
 // to turn sigma into N_hat, instead of two of each.
 //
 // One RK stage i of step n is three launches (two with Raman off):
-//   k_pair      per pair field (l<=m):  V = U_l conj(U_m) -> FFT -> * H_R -> IFFT,
-//                                       W = (1-fR) V + result          (Raman on only)
-//   k_contract  per time tile:          sigma_p = sum Q U_k W_lm        (all p)
+//   k_pair      per pair field (l<=m):  V = U_l conj(U_m) -> FFT -> * H_R -> IFFT = R
+//                                                                       (Raman on only)
+//   k_contract  per time tile:          sigma_p = sum Q U_k [(1-fR) U_l conj(U_m) + R_lm]
+//                                       (all p; Raman off: sum Q U_k U_l conj(U_m))
 //   k_nu        per mode p:             FFT(sigma_p) -> N_hat_i = i sgn(gamma) conj(E_i) *.,
 //                                       [last stage: psi_hat += h sum b_j N_hat_j, monitors],
 //                                       x_hat = psi_hat + h sum a_{i+1,j} N_hat_j,
@@ -20,6 +21,8 @@
 // is never stored: the phase Im L_p(w) * (z_n + c_i h) is evaluated in FP64,
 // reduced mod 2 pi in FP64 and only then passed to sincos in T.
 #pragma once
+
+#include <type_traits>
 
 #include "fft.cuh"
 
@@ -74,6 +77,29 @@ __device__ __forceinline__ void load_poly(double* poly, const SolveDesc& d, int 
   __syncthreads();
 }
 
+// One warp copies this CTA's solve descriptor into shared memory in a single round
+// trip, instead of every field becoming its own dependent global load. The caller
+// synchronises before reading it.
+static_assert(sizeof(SolveDesc) % 8 == 0, "descriptor copied in 8-byte words");
+__device__ __forceinline__ void stage_desc(SolveDesc* dst, const SolveDesc* src) {
+  constexpr int W = (int)(sizeof(SolveDesc) / 8);
+  if (threadIdx.x < W)
+    reinterpret_cast<unsigned long long*>(dst)[threadIdx.x] =
+        __ldg(reinterpret_cast<const unsigned long long*>(src) + threadIdx.x);
+}
+
+// Ask the TMA engine to pull [p, p + bytes) into L2 without waiting for it
+// (p 16-byte aligned, bytes a multiple of 16). Used to have a row ready in L2 by the
+// time a kernel's epilogue reads it.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  constexpr unsigned kPiece = 64u * 1024u;
+  const char* c = static_cast<const char*>(p);
+  for (unsigned off = 0; off < bytes; off += kPiece) {
+    const unsigned n = bytes - off < kPiece ? bytes - off : kPiece;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + off), "r"(n) : "memory");
+  }
+}
+
 template <typename G> __device__ __forceinline__ int cluster_rank() {
   if constexpr (G::C == 1) return 0;
   else return (int)cg::this_cluster().block_rank();
@@ -85,21 +111,24 @@ template <typename G> __device__ __forceinline__ int cluster_rank() {
   V* s = reinterpret_cast<V*>(smem_raw);
 
 // ---- k_prime: U for stage `stage` from psi_hat (and the stored N_hat_j) -------------------
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_prime(const KParams kp) {
-  using Gm = Geo<T, LOGN>;
+template <typename T, int LOGN, int XC>
+__global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_prime(const KParams kp) {
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
-  const SolveDesc& d = kp.descs[blockIdx.y];
+  __shared__ SolveDesc sdesc;
+  stage_desc(&sdesc, kp.descs + blockIdx.y);
+  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, kp.tw);
+  __syncthreads();
+  const SolveDesc& d = sdesc;
   const int p = blockIdx.x / Gm::C;
   if (p >= d.M) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
-  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
   const int i = kp.stage;
-  const unsigned long long n = *((volatile unsigned long long*)d.step);
+  const unsigned long long n = __ldcg(d.step);
   const double zs = ((double)n + kp.tab.c[i]) * d.dz;
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
@@ -119,80 +148,233 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_prime(const KParams k
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * zs;
     s[pad(li)] = cmul(from_d2<T>(x), expi<T>(th));
   }
-  inverse<T, LOGN>(s, sq, kp.tw);
+  inverse<T, LOGN, XC>(s, sq, kp.tw);
   V* U = as_t2<T>(d.U);
   const T inv = (T)d.inv_nt;
 #pragma unroll 8
   for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[row + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
 }
 
-// ---- k_pair: W_q = (1 - fR) V_q + IFFT(FFT(V_q) * H), V_q = U_l conj(U_m) ----------------
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_pair(const KParams kp) {
-  using Gm = Geo<T, LOGN>;
+// ---- k_pair: R_q = IFFT(FFT(V_q) * H), V_q = U_l conj(U_m) -------------------------------
+template <typename T, int LOGN, int XC>
+__global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_pair(const KParams kp) {
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   MMP_ROW_SMEM();
-  const SolveDesc& d = kp.descs[blockIdx.y];
+  __shared__ SolveDesc sdesc;
+  stage_desc(&sdesc, kp.descs + blockIdx.y);
+  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, kp.tw);
+  __syncthreads();
+  const SolveDesc& d = sdesc;
   const int q = blockIdx.x / Gm::C;
-  if (q >= d.P) return;
+  if (q >= d.P) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
-  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   const int2 lm = d.pairs[q];
   const V* U = as_t2<T>(d.U);
   const size_t rl = (size_t)lm.x * Gm::N, rm = (size_t)lm.y * Gm::N;
+  if constexpr (Gm::C == 1 && sizeof(T) == 4) {
+    // one CTA per row: two consecutive samples per 16-byte load
+    const float4* Ul = reinterpret_cast<const float4*>(U + rl);
+    const float4* Um = reinterpret_cast<const float4*>(U + rm);
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
-    const int t = Gm::time_of(rank, u);
-    s[pad(u)] = cmulc(U[rl + t], U[rm + t]);
+    for (int u2 = tid; u2 < Gm::NL / 2; u2 += Gm::NTHR) {
+      const float4 a = Ul[u2], b = Um[u2];
+      s[pad(2 * u2)] = cmulc(make_float2(a.x, a.y), make_float2(b.x, b.y));
+      s[pad(2 * u2 + 1)] = cmulc(make_float2(a.z, a.w), make_float2(b.z, b.w));
+    }
+  } else {
+#pragma unroll 8
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
+      const int t = Gm::time_of(rank, u);
+      s[pad(u)] = cmulc(U[rl + t], U[rm + t]);
+    }
   }
-  forward<T, LOGN>(s, sq, kp.tw);
+  forward<T, LOGN, XC>(s, sq, kp.tw);
   const V* H = as_t2<T>(d.H);
-#pragma unroll 4
-  for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = cmul(s[pad(li)], __ldg(&H[Gm::freq_of(rank, li)]));
-  inverse<T, LOGN>(s, sq, kp.tw);
-  V* W = as_t2<T>(d.W) + (size_t)q * Gm::N;
-  const T kerr = (T)d.one_minus_fR;
-  // V is formed again from U (L2-resident) instead of being kept across both transforms
+  if constexpr (Gm::C == 1 && sizeof(T) == 4) {
+    const float4* H4 = reinterpret_cast<const float4*>(H);
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
-    const int t = Gm::time_of(rank, u);
-    W[t] = cadd(cscale(cmulc(U[rl + t], U[rm + t]), kerr), s[pad(u)]);
+    for (int k2 = tid; k2 < Gm::NL / 2; k2 += Gm::NTHR) {
+      const float4 hh = __ldg(&H4[k2]);
+      s[pad(2 * k2)] = cmul(s[pad(2 * k2)], make_float2(hh.x, hh.y));
+      s[pad(2 * k2 + 1)] = cmul(s[pad(2 * k2 + 1)], make_float2(hh.z, hh.w));
+    }
+  } else {
+#pragma unroll 4
+    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = cmul(s[pad(li)], __ldg(&H[Gm::freq_of(rank, li)]));
   }
+  inverse<T, LOGN, XC>(s, sq, kp.tw);
+  // R_q = (H_R conv V_q); the Kerr part (1 - fR) V_q is formed by the contraction from
+  // the U tile it already holds
+  V* R = as_t2<T>(d.W) + (size_t)q * Gm::N;
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) R[Gm::time_of(rank, u)] = s[pad(u)];
 }
 
 // ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) {
-  using Gm = Geo<T, LOGN>;
+template <typename T, int LOGN, int XC>
+__global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_nu(const KParams kp) {
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
   __shared__ double red[2][32];
-  const SolveDesc& d = kp.descs[blockIdx.y];
+  __shared__ SolveDesc sdesc;
+  stage_desc(&sdesc, kp.descs + blockIdx.y);
+  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, kp.tw);
+  __syncthreads();
+  const SolveDesc& d = sdesc;
   const int p = blockIdx.x / Gm::C;
-  if (p >= d.M) return;
+  if (p >= d.M) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
-  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
+  // Scalars needed after the forward transform live in shared memory rather than in
+  // registers, so the (out-of-line) transform call has little to save and restore.
+  __shared__ unsigned long long s_cnt[2];  // step since z reset, steps since creation
+  __shared__ double s_z[2];               // z at this stage, z at the next stage
+  // Stage-combination list: the stored N_hat_j entering x_hat (or, at the last stage,
+  // psi_{n+1} = psi_n + h sum_j b_j N_j, src/MultimodePropagation_CPU.cpp:75-85) with
+  // their coefficients h*a or h*b; N_hat_i itself comes from registers (cself).
+  // Thread 0 also starts L2 prefetches of the psi_hat and N_hat_j spans this CTA
+  // reads after its forward transform, so they arrive while the transform runs.
+  __shared__ int s_jq[kMaxStages];
+  __shared__ double s_cq[kMaxStages];
+  __shared__ int s_nq;
+  if (tid == 0) {
+    const int i = kp.stage;
+    const int S = kp.tab.s;
+    const bool last = (i == S - 1);
+    const double h = d.dz;
+    const size_t row = (size_t)p * Gm::N;
+    const size_t mstride = (size_t)d.M * Gm::N;
+    const V* Nh = as_t2<T>(d.Nh);
+    const unsigned long long n = __ldcg(d.step);
+    s_cnt[0] = n;
+    s_cnt[1] = __ldcg(d.total);
+    s_z[0] = ((double)n + kp.tab.c[i]) * h;
+    s_z[1] = last ? ((double)(n + 1)) * h : ((double)n + kp.tab.c[i + 1]) * h;
+    int nq = 0;
+    if (last) {
+      for (int j = 0; j < S; ++j)
+        if (j != i && kp.tab.b[j] != 0.0) { s_jq[nq] = j; s_cq[nq] = kp.tab.b[j] * h; ++nq; }
+    } else {
+      for (int j = 0; j < i; ++j)
+        if (kp.tab.a[i + 1][j] != 0.0) { s_jq[nq] = j; s_cq[nq] = kp.tab.a[i + 1][j] * h; ++nq; }
+    }
+    s_nq = nq;
+    for (int qb = 0; qb < Gm::C; ++qb) {  // the CTA's frequencies: C spans of CH
+      const size_t f0 = row + (size_t)rank * Gm::CH + (size_t)Gm::NL * qb;
+      prefetch_l2(d.psi_hat + f0, Gm::CH * (unsigned)sizeof(double2));
+      for (int q = 0; q < nq; ++q) prefetch_l2(Nh + (size_t)s_jq[q] * mstride + f0, Gm::CH * (unsigned)sizeof(V));
+    }
+  }
+  const V* sig = as_t2<T>(d.sigma);
+  if constexpr (Gm::C == 1 && sizeof(T) == 4) {
+    const float4* sg = reinterpret_cast<const float4*>(sig + (size_t)p * Gm::N);
+#pragma unroll 8
+    for (int u2 = tid; u2 < Gm::NL / 2; u2 += Gm::NTHR) {
+      const float4 a = sg[u2];
+      s[pad(2 * u2)] = make_float2(a.x, a.y);
+      s[pad(2 * u2 + 1)] = make_float2(a.z, a.w);
+    }
+  } else {
+#pragma unroll 8
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = sig[(size_t)p * Gm::N + Gm::time_of(rank, u)];
+  }
+  forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers also publish the values thread 0 wrote
   const int i = kp.stage;
   const int S = kp.tab.s;
   const bool last = (i == S - 1);
-  const unsigned long long n = *((volatile unsigned long long*)d.step);
-  const unsigned long long total = *((volatile unsigned long long*)d.total);
-  const double zi = ((double)n + kp.tab.c[i]) * d.dz;
-  const double znext = last ? ((double)(n + 1)) * d.dz : ((double)n + kp.tab.c[i + 1]) * d.dz;
+  const double h = d.dz;
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
-  const V* sig = as_t2<T>(d.sigma);
-#pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = sig[row + Gm::time_of(rank, u)];
-  forward<T, LOGN>(s, sq, kp.tw);
   V* Nh = as_t2<T>(d.Nh);
-  const double h = d.dz;
+  const double zi = s_z[0], znext = s_z[1];
   double e_part = 0.0, p_part = 0.0;
   bool finite = true;
+  const int nq = s_nq;
+  const double cself = (last ? kp.tab.b[i] : kp.tab.a[i + 1][i]) * h;
+  constexpr int MAXQ = 6;
+  // Fast path, one body per count of stored terms (no predicated dead work): all loads
+  // of a chunk of frequencies are issued before its math. Intermediate stages combine
+  // x_hat in T (it only feeds the nonlinearity, which runs in T); the last stage
+  // accumulates psi_{n+1} in FP64.
+  auto body = [&](auto nqc) {
+    constexpr int NQ = decltype(nqc)::value;
+    constexpr int CHK = 2 < Gm::E ? 2 : Gm::E;
+    const double nb3 = d.n_beta == 3;
+#pragma unroll 1
+    for (int e0 = 0; e0 < Gm::E; e0 += CHK) {
+      int kk[CHK];
+      double2 ps[CHK];
+      V sv[CHK];
+      V nj[CHK][NQ > 0 ? NQ : 1];
+#pragma unroll
+      for (int c = 0; c < CHK; ++c) {
+        const int li = tid + (e0 + c) * Gm::NTHR;
+        kk[c] = Gm::freq_of(rank, li);
+        ps[c] = d.psi_hat[row + kk[c]];
+        sv[c] = s[pad(li)];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) nj[c][q] = Nh[(size_t)s_jq[q] * mstride + row + kk[c]];
+      }
+#pragma unroll
+      for (int c = 0; c < CHK; ++c) {
+        const int li = tid + (e0 + c) * Gm::NTHR;
+        const int k = kk[c];
+        const double alpha = alpha_of(k, Gm::N, d.alpha_scale);
+        const double L = nb3 ? fma(fma(poly[2], alpha, poly[1]), alpha, poly[0]) : im_L(poly, d.n_beta, alpha);
+        // N_hat_i = i sgn(gamma) conj(E_i) FFT(sigma)   (src/MultimodePropagation_CPU.cpp:231-237)
+        const V xe = cmulc(sv[c], expi<T>(L * zi));
+        V nh;
+        nh.x = (T)(-d.sgn_gamma) * xe.y;
+        nh.y = (T)(d.sgn_gamma) * xe.x;
+        Nh[(size_t)i * mstride + row + k] = nh;
+        V xt;
+        if (last) {
+          const double2 nhd = to_d2(nh);
+          double2 x = ps[c];
+          x.x = fma(cself, nhd.x, x.x);
+          x.y = fma(cself, nhd.y, x.y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) {
+            const double2 v = to_d2(nj[c][q]);
+            x.x = fma(s_cq[q], v.x, x.x);
+            x.y = fma(s_cq[q], v.y, x.y);
+          }
+          d.psi_hat[row + k] = x;
+          const double a2 = x.x * x.x + x.y * x.y;
+          finite = finite && isfinite(a2);
+          e_part += a2;
+          if (d.omega0_T0 != 0.0) p_part += a2 / (d.omega0_T0 + alpha);
+          xt = from_d2<T>(x);
+        } else {
+          xt = from_d2<T>(ps[c]);
+          const T cs = (T)cself;
+          xt.x = fma(cs, nh.x, xt.x);
+          xt.y = fma(cs, nh.y, xt.y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) {
+            const T cq = (T)s_cq[q];
+            xt.x = fma(cq, nj[c][q].x, xt.x);
+            xt.y = fma(cq, nj[c][q].y, xt.y);
+          }
+        }
+        s[pad(li)] = cmul(xt, expi<T>(L * znext));
+      }
+    }
+  };
+  // Only the counts RK4 needs (0 at intermediate stages, 3 at the last) get their own
+  // body: every extra copy of this loop grows the kernel, and a larger kernel pushes the
+  // transform code out of the instruction cache between calls (measured: the forward
+  // transform ran ~50% slower with seven copies). Other tableaus take the generic loop.
+  if (nq == 0) {
+    body(std::integral_constant<int, 0>{});
+  } else if (nq == 3) {
+    body(std::integral_constant<int, 3>{});
+  } else {
 #pragma unroll 2
   for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
     const int k = Gm::freq_of(rank, li);
@@ -233,13 +415,12 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
     }
     s[pad(li)] = cmul(from_d2<T>(x), expi<T>(L * znext));
   }
-  inverse<T, LOGN>(s, sq, kp.tw);
-  V* U = as_t2<T>(d.U);
-  const T inv = (T)d.inv_nt;
-#pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[row + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
+  }
   if (last) {
-    // block reduction of the monitors, then the last CTA of this solve advances the step
+    // Block reduction of the monitors, then the last CTA of this solve advances the
+    // step. Done before the inverse transform, so none of it is live across that call;
+    // every CTA of the solve read the step counter at its start, and the next launch
+    // starts only after this one has finished.
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       e_part += __shfl_xor_sync(0xffffffffu, e_part, o);
@@ -249,6 +430,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
     if ((tid & 31) == 0) { red[0][tid >> 5] = e_part; red[1][tid >> 5] = p_part; }
     __syncthreads();
     if (tid == 0) {
+      const unsigned long long n = s_cnt[0], total = s_cnt[1];
       double es = 0.0, ps = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { es += red[0][w]; ps += red[1][w]; }
       if (!finite_all) atomicOr(d.status, kStatusNonFinite);
@@ -266,23 +448,31 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_nu(const KParams kp) 
       }
     }
   }
+  inverse<T, LOGN, XC>(s, sq, kp.tw);
+  V* U = as_t2<T>(d.U);
+  const T inv = (T)d.inv_nt;
+#pragma unroll 8
+  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[(size_t)p * Gm::N + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
 }
 
 // ---- k_result: phi_p = IFFT(exp(L_p z) psi_hat_p) / conversion_factor -> io (FP64) --------
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_result(const KParams kp) {
-  using Gm = Geo<T, LOGN>;
+template <typename T, int LOGN, int XC>
+__global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_result(const KParams kp) {
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   MMP_ROW_SMEM();
   __shared__ double poly[kMaxBeta];
-  const SolveDesc& d = kp.descs[blockIdx.y];
+  __shared__ SolveDesc sdesc;
+  stage_desc(&sdesc, kp.descs + blockIdx.y);
+  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, kp.tw);
+  __syncthreads();
+  const SolveDesc& d = sdesc;
   const int p = blockIdx.x / Gm::C;
-  if (p >= d.M) return;
+  if (p >= d.M) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
-  const V* sq = load_twiddles<T, LOGN>(smem_raw, kp.tw);
   load_poly(poly, d, p);
-  const unsigned long long n = *((volatile unsigned long long*)d.step);
+  const unsigned long long n = __ldcg(d.step);
   const double z = (double)n * d.dz;
   const size_t row = (size_t)p * Gm::N;
 #pragma unroll 2
@@ -291,7 +481,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_result(const KParams 
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * z;
     s[pad(li)] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
   }
-  inverse<T, LOGN>(s, sq, kp.tw);
+  inverse<T, LOGN, XC>(s, sq, kp.tw);
 #pragma unroll 8
   for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
     const double2 r = to_d2(s[pad(u)]);
@@ -310,21 +500,21 @@ struct DftArgs {
   TwTables tw;
 };
 
-template <typename T, int LOGN, bool INV>
-__global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_dft(const DftArgs a) {
-  using Gm = Geo<T, LOGN>;
+template <typename T, int LOGN, int XC, bool INV>
+__global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_dft(const DftArgs a) {
+  using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   MMP_ROW_SMEM();
   const int r = blockIdx.x / Gm::C;
   if (r >= a.rows) return;
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
-  const V* sq = load_twiddles<T, LOGN>(smem_raw, a.tw);
+  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, a.tw);
   const size_t row = (size_t)r * Gm::N;
   if constexpr (!INV) {
 #pragma unroll 8
     for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = from_d2<T>(a.in[row + Gm::time_of(rank, u)]);
-    forward<T, LOGN>(s, sq, a.tw);
+    forward<T, LOGN, XC>(s, sq, a.tw);
 #pragma unroll 8
     for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
       const double2 x = to_d2(s[pad(li)]);
@@ -333,7 +523,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN>::NTHR, 1) k_dft(const DftArgs a) 
   } else {
 #pragma unroll 8
     for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = from_d2<T>(a.in[row + Gm::freq_of(rank, li)]);
-    inverse<T, LOGN>(s, sq, a.tw);
+    inverse<T, LOGN, XC>(s, sq, a.tw);
 #pragma unroll 8
     for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
       const double2 x = to_d2(s[pad(u)]);
@@ -397,6 +587,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   const int M = d.M;
   const int raman = d.raman;
   const int P = raman ? d.P : 0;
+  const T kerr = (T)d.one_minus_fR;
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
   const Term* terms = d.terms;
@@ -433,12 +624,11 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
     const int j1 = d.term_off[p + 1];
     for (int j = d.term_off[p]; j < j1; ++j) {
       const Term tm = terms[j];
-      V w;
+      V w = cmulc(sU[tm.l * TT + tt], sU[tm.m * TT + tt]);
       if (raman) {
-        w = sW[tm.a * TT + tt];
-        if (tm.conj) w.y = -w.y;
-      } else {
-        w = cmulc(sU[tm.a * TT + tt], sU[tm.b * TT + tt]);
+        V r = sW[(tm.pc & 0x7fff) * TT + tt];
+        if (tm.pc & 0x8000) r.y = -r.y;
+        w = cadd(cscale(w, kerr), r);
       }
       const V uw = cmul(sU[tm.k * TT + tt], w);
       const T qv = (T)tm.q;
