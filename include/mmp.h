@@ -170,6 +170,41 @@ int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info);
 uint32_t mmp_batch_size(const mmp_batch* b);
 void mmp_batch_destroy(mmp_batch* b);
 
+/* ---- serving: a request loop with continuous batching ---------------------------------
+ * No counterpart in the reference (one solve per process). A worker thread owns the
+ * device. Requests are grouped by kernel shape (nt, precision, Raman, RK tableau) into
+ * slot pools; each pool advances all its solves with one captured multi-step CUDA
+ * graph per replay on its own stream, so different pools overlap on the device.
+ * Between replays the worker retires finished solves (their result is copied to host
+ * memory) and admits waiting ones into free slots, first fit, as long as the device
+ * memory they need stays within the budget. Each solve stops at its own n_steps on
+ * the device. Results equal those of mmp_solver_create + mmp_propagate(n_steps) +
+ * mmp_get_result for the same parameters. */
+typedef struct mmp_server mmp_server;
+typedef struct mmp_server_config {
+  uint64_t memory_budget;   /* device bytes for solve state; 0 = 80% of free memory */
+  uint32_t max_slots;       /* solves per pool; 0 = 64 */
+  uint32_t steps_per_tick;  /* RK steps per graph replay; 0 = 32 */
+  uint32_t flags;           /* MMP_F_* OR-ed into every request's flags */
+} mmp_server_config;
+typedef struct mmp_request_info {
+  int32_t status;           /* MMP_OK, or the error the solve ended with */
+  uint32_t n_modes, nt;
+  uint64_t steps;           /* RK steps run */
+  double submit_s, start_s, done_s; /* seconds since the server was created */
+} mmp_request_info;
+int mmp_server_create(const mmp_server_config* cfg, mmp_server** out);
+/* Copies the parameters (and their arrays); returns at once with a request id. */
+int mmp_server_submit(mmp_server* s, const mmp_params* params, uint64_t* id);
+/* *done = 1 once the request has finished (successfully or not). */
+int mmp_server_poll(mmp_server* s, uint64_t id, int* done);
+/* Wait up to timeout_s seconds (< 0: no limit) for the request; then copy its result
+ * phi[M][NT][2] into out (if not NULL) and its info, and forget the request.
+ * MMP_ETIMEOUT if it did not finish in time (it stays queued). */
+int mmp_server_wait(mmp_server* s, uint64_t id, double timeout_s, double* out, mmp_request_info* info);
+/* Stops the worker; unfinished requests are dropped. NULL is allowed. */
+void mmp_server_destroy(mmp_server* s);
+
 /* ---- measurement (no counterpart in the reference, which has no timing code) --------- */
 /* `repeats` calls of mmp_batch_propagate_async(b, nz) bracketed by CUDA events on the
  * batch's own stream; *ms receives the device time between the events. */

@@ -21,7 +21,7 @@ from . import capi, workloads  # noqa: F401
 from .capi import (MMP_F_CONTINUOUS, MMP_F_FP64, MMP_F_NO_MONITORS,  # noqa: F401
                    MMP_F_PHYSICAL_PAIRS, MMP_RK_BUTCHER7_LAMBDA_MU, MMP_RK_BY_ORDER)
 
-__all__ = ["Solver", "Batch", "MMPError", "dft", "lib", "workloads", "capi"]
+__all__ = ["Solver", "Batch", "Server", "MMPError", "dft", "lib", "workloads", "capi"]
 
 
 class MMPError(RuntimeError):
@@ -189,6 +189,62 @@ class Batch:
     def close(self):
         if self._ptr:
             lib().mmp_batch_destroy(self._ptr)
+            self._ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop with continuous batching: submit whole solves (each runs its own
+    n_steps from its initial fields); a device worker admits them into slot pools of
+    their kernel shape as memory allows, advances every pool steps_per_tick steps per
+    replay and retires finished solves. Results equal a standalone Solver's."""
+
+    def __init__(self, memory_budget: int = 0, max_slots: int = 0, steps_per_tick: int = 0,
+                 flags: int = 0):
+        cfg = capi.mmp_server_config(memory_budget, max_slots, steps_per_tick, flags)
+        self._ptr = C.c_void_p()
+        _check(lib().mmp_server_create(C.byref(cfg), C.byref(self._ptr)), "mmp_server_create")
+        self._shape = {}
+
+    def submit(self, prob) -> int:
+        h = prob.to_params()
+        rid = C.c_uint64(0)
+        _check(lib().mmp_server_submit(self._ptr, h.ptr(), C.byref(rid)), "mmp_server_submit")
+        self._shape[rid.value] = (prob.n_modes, prob.nt)
+        return rid.value
+
+    def done(self, rid: int) -> bool:
+        d = C.c_int(0)
+        _check(lib().mmp_server_poll(self._ptr, rid, C.byref(d)), "mmp_server_poll")
+        return bool(d.value)
+
+    def wait(self, rid: int, timeout: float | None = None):
+        """(fields complex128 [M][NT], info dict with status, steps and the submit /
+        start / done times in seconds since the server started)."""
+        M, nt = self._shape[rid]
+        out = np.empty((M, nt), dtype=np.complex128)
+        info = capi.mmp_request_info()
+        rc = lib().mmp_server_wait(self._ptr, rid, -1.0 if timeout is None else float(timeout),
+                                   _dptr(out.view(np.float64)), C.byref(info))
+        if info.nt != 0:  # info is filled once the request finished; the server then forgets it
+            self._shape.pop(rid, None)
+        _check(rc, "mmp_server_wait")
+        return out, {name: getattr(info, name) for name, _ in info._fields_}
+
+    def close(self):
+        if self._ptr:
+            lib().mmp_server_destroy(self._ptr)
             self._ptr = C.c_void_p()
 
     def __enter__(self):

@@ -77,6 +77,21 @@ class mmp_info(C.Structure):
     ]
 
 
+class mmp_server_config(C.Structure):
+    _fields_ = [
+        ("memory_budget", C.c_uint64), ("max_slots", C.c_uint32),
+        ("steps_per_tick", C.c_uint32), ("flags", C.c_uint32),
+    ]
+
+
+class mmp_request_info(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("n_modes", C.c_uint32), ("nt", C.c_uint32),
+        ("steps", C.c_uint64),
+        ("submit_s", C.c_double), ("start_s", C.c_double), ("done_s", C.c_double),
+    ]
+
+
 # name -> (restype, argtypes); every symbol include/mmp.h declares
 SIGNATURES = {
     "mmp_validate_params": (C.c_int, [C.POINTER(mmp_params), C.c_char_p, C.c_size_t]),
@@ -110,6 +125,12 @@ SIGNATURES = {
                          C.POINTER(C.c_double)]),
     "mmp_dft_noalloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]),
+    "mmp_server_create": (C.c_int, [C.POINTER(mmp_server_config), C.POINTER(C.c_void_p)]),
+    "mmp_server_submit": (C.c_int, [C.c_void_p, C.POINTER(mmp_params), C.POINTER(C.c_uint64)]),
+    "mmp_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
+    "mmp_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_double),
+                                  C.POINTER(mmp_request_info)]),
+    "mmp_server_destroy": (None, [C.c_void_p]),
     "mmp_strerror": (C.c_char_p, [C.c_int]),
     "mmp_last_error": (C.c_char_p, []),
     "mmp_version": (C.c_char_p, []),

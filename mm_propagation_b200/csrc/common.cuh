@@ -110,6 +110,9 @@ struct SolveDesc {
   int* status;                // bit 0: non-finite field seen
   int monitors;               // 1: accumulate monitors
   int pad_;
+  // Stage kernels do nothing for this solve once *step >= step_limit (a solve in a
+  // served pool stops at its own step count while the pool's graph keeps running).
+  unsigned long long step_limit;
 };
 
 // RK tableau passed by value to the stage kernels (identical for a batch).

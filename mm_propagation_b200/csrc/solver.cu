@@ -280,6 +280,7 @@ struct Member {
   unsigned long long mon_cap = 0;
   unsigned long long total_host = 0;  // steps enqueued since creation
   unsigned long long step_host = 0;   // steps since the last z reset
+  size_t bytes = 0;                   // device bytes of `block`
 };
 
 int validate(const mmp_params* p, std::string& why) {
@@ -435,8 +436,14 @@ struct mmp_batch {
   uint32_t nt = 0;
   int logn = 0;
   Tableau tab{};
+  // Slots: `capacity` descriptors on the device; members[i] is in use when active[i].
+  // An ordinary batch fills every slot; a served pool admits and retires solves
+  // between graph replays, and the kernels skip empty slots (M = 0).
+  uint32_t capacity = 0;
   std::vector<Member> members;
+  std::vector<uint8_t> active;
   SolveDesc* d_descs = nullptr;
+  uint32_t span = 0;  // slots the kernels are launched over: highest active slot + 1
   int Mmax = 0, Pmax = 0;
   int TT = 32;
   int stage_terms = 0;
@@ -457,10 +464,17 @@ namespace {
 void* T2ptr(void* base, size_t off) { return (char*)base + off; }
 
 int upload_desc(mmp_batch* b) {
-  std::vector<SolveDesc> h(b->members.size());
-  for (size_t i = 0; i < b->members.size(); ++i) h[i] = b->members[i].desc;
+  std::vector<SolveDesc> h(b->capacity);
+  for (size_t i = 0; i < b->capacity; ++i) {
+    if (b->active[i]) {
+      h[i] = b->members[i].desc;
+    } else {
+      std::memset(&h[i], 0, sizeof(SolveDesc));  // empty slot: M = 0, every kernel skips it
+    }
+  }
   CUDA_TRY(cudaMemcpyAsync(b->d_descs, h.data(), h.size() * sizeof(SolveDesc), cudaMemcpyHostToDevice,
                            b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));  // h is a host temporary
   return MMP_OK;
 }
 
@@ -512,7 +526,7 @@ int launch_contract(mmp_batch* b) {
   const SolveDesc* descs = b->d_descs;
   int nt = (int)b->nt, TT = b->TT, st = b->stage_terms;
   void* args[] = {(void*)&descs, &nt, &TT, &st};
-  dim3 grid((unsigned)(b->nt / b->TT), (unsigned)b->members.size(), 1);
+  dim3 grid((unsigned)(b->nt / b->TT), b->span, 1);
   const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, b->stream, args));
   return MMP_OK;
@@ -526,7 +540,7 @@ std::mutex g_tune_mu;
 std::map<std::vector<int>, int> g_tune_cache;
 
 int time_variant(mmp_batch* b, const KernelSet& ks, float* ms) {
-  const int nsol = (int)b->members.size();
+  const int nsol = (int)b->span;
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
@@ -579,7 +593,7 @@ int autotune(mmp_batch* b) {
 }
 
 int enqueue_step(mmp_batch* b) {
-  const int nsol = (int)b->members.size();
+  const int nsol = (int)b->span;
   for (int i = 0; i < b->tab.s; ++i) {
     int rc;
     if (b->raman && b->Pmax > 0) {
@@ -622,6 +636,7 @@ int build_graph(mmp_batch* b, int steps) {
 int check_status(mmp_batch* b) {
   int bad = 0;
   for (auto& s : b->members) {
+    if (!s.block) continue;  // empty slot
     int st = 0;
     CUDA_TRY(cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
                         cudaMemcpyDeviceToHost));
@@ -636,6 +651,7 @@ int batch_propagate_async(mmp_batch* b, uint32_t nz) {
   if (!b) return fail(MMP_EINVAL, "NULL batch");
   CUDA_TRY(cudaSetDevice(b->device));
   for (auto& s : b->members) {
+    if (!s.block) continue;  // empty slot
     const bool continuous = (s.flags & MMP_F_CONTINUOUS) != 0;
     if (!continuous) {
       // initLawsonRK: z = 0 (src/MultimodePropagation.cpp:158-163)
@@ -649,7 +665,7 @@ int batch_propagate_async(mmp_batch* b, uint32_t nz) {
   }
   if (nz == 0) return MMP_OK;
   // U for stage 0 at the current z
-  int rc = launch_row_kernel(b, b->ks, b->ks.prime, b->Mmax, (int)b->members.size(), 0, b->d_descs);
+  int rc = launch_row_kernel(b, b->ks, b->ks.prime, b->Mmax, (int)b->span, 0, b->d_descs);
   if (rc) return rc;
   const int G = 8;  // steps per captured graph
   uint32_t left = nz;
@@ -716,33 +732,13 @@ int member_set_fields(mmp_batch* b, uint32_t idx, const double* phi0) {
   return MMP_OK;
 }
 
-int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
-  if (!out) return fail(MMP_EINVAL, "out is NULL");
-  *out = nullptr;
-  if (!params || n == 0) return fail(MMP_EINVAL, "empty batch");
-  for (uint32_t i = 0; i < n; ++i) {
-    std::string why;
-    int rc = validate(params[i], why);
-    if (rc) return fail(rc, "member " + std::to_string(i) + ": " + why);
-  }
-  const mmp_params* p0 = params[0];
-  Tableau tab0;
-  tableau_for(p0, tab0);
-  for (uint32_t i = 1; i < n; ++i) {
-    const mmp_params* p = params[i];
-    Tableau t;
-    tableau_for(p, t);
-    if (p->nt != p0->nt || (p->flags & MMP_F_FP64) != (p0->flags & MMP_F_FP64) ||
-        (p->raman != 0) != (p0->raman != 0) || std::memcmp(&t, &tab0, sizeof(t)) != 0)
-      return fail(MMP_EINVAL, "batch members must share nt, precision, raman and the RK tableau");
-  }
+// Batch-wide state every member shares: device resources, kernel sets, stream.
+int batch_open(mmp_batch* b, const mmp_params* p0, const Tableau& tab0) {
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   DeviceRes* res = nullptr;
   int rc = ensure_device(dev, &res);
   if (rc) return rc;
-
-  mmp_batch* b = new mmp_batch();
   b->device = dev;
   b->dev = res;
   b->fp64 = (p0->flags & MMP_F_FP64) != 0;
@@ -752,95 +748,111 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
   b->tab = tab0;
   b->ks = kernels_for(b->fp64 ? 1 : 0, b->logn);
   b->ks64 = kernels_for(1, b->logn);
-  if (!b->ks.prime || !b->ks64.prime) {
-    delete b;
-    return fail(MMP_ENOTSUP, "no kernels built for this nt");
-  }
+  if (!b->ks.prime || !b->ks64.prime) return fail(MMP_ENOTSUP, "no kernels built for this nt");
   b->kernels_per_step = b->tab.s * ((b->raman ? 1 : 0) + 2);
-  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) {
-    delete b;
-    return fail(MMP_ECUDA, cudaGetErrorString(e));
-  }
-  b->members.resize(n);
+  CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaMalloc(&b->d_descs, (size_t)b->capacity * sizeof(SolveDesc)));
+  return MMP_OK;
+}
+
+bool same_shape(const mmp_batch* b, const mmp_params* p) {
+  Tableau t;
+  tableau_for(p, t);
+  return p->nt == b->nt && ((p->flags & MMP_F_FP64) != 0) == b->fp64 && (p->raman != 0) == b->raman &&
+         std::memcmp(&t, &b->tab, sizeof(t)) == 0;
+}
+
+size_t member_bytes(const mmp_batch* b, const Member& s) {
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
-  const size_t nt = b->nt;
-  int build_rc = MMP_OK;
-  for (uint32_t i = 0; i < n && build_rc == MMP_OK; ++i) {
-    Member& s = b->members[i];
-    host_setup(params[i], s);
-    const size_t M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
-    // one allocation: psi_hat | io | Nh | U | sigma | W | H | poly | pairs | terms | term_off | counters
-    size_t off = 0;
-    const size_t o_psi = off; off = align_up(off + M * nt * sizeof(double2));
-    const size_t o_io = off; off = align_up(off + M * nt * sizeof(double2));
-    const size_t o_nh = off; off = align_up(off + S * M * nt * t2);
-    const size_t o_u = off; off = align_up(off + M * nt * t2);
-    const size_t o_sig = off; off = align_up(off + M * nt * t2);
-    const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
-    const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
-    const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
-    const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
-    const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
-    const size_t o_toff = off; off = align_up(off + (M + 1) * sizeof(int));
-    const size_t o_cnt = off; off = align_up(off + 4 * sizeof(unsigned long long));
-    e = cudaMalloc(&s.block, off);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ENOMEM, "cudaMalloc solver state: " + std::string(cudaGetErrorString(e))); break; }
-    e = cudaMemsetAsync(s.block, 0, off, b->stream);
-    SolveDesc& d = s.desc;
-    std::memset(&d, 0, sizeof(d));
-    d.M = (int)M;
-    d.P = (int)P;
-    d.n_beta = (int)s.n_beta;
-    d.raman = b->raman ? 1 : 0;
-    d.alpha_scale = 2 * M_PI / s.t_final;
-    d.dz = s.delta_z;
-    d.sgn_gamma = s.sgn_gamma;
-    d.one_minus_fR = b->raman ? (1.0 - s.fR) : 1.0;
-    d.inv_nt = 1.0 / (double)nt;
-    d.result_scale = 1.0 / ((double)nt * s.cf);
-    d.energy_scale = s.delta_t * s.T0 / (s.cf * s.cf * (double)nt);
-    d.omega0_T0 = s.omega0 * s.T0;
-    d.photon_scale = d.energy_scale * s.T0 / 1.054571817e-10;
-    d.poly = (const double*)T2ptr(s.block, o_poly);
-    d.psi_hat = (double2*)T2ptr(s.block, o_psi);
-    d.io = (double2*)T2ptr(s.block, o_io);
-    d.Nh = T2ptr(s.block, o_nh);
-    d.U = T2ptr(s.block, o_u);
-    d.sigma = T2ptr(s.block, o_sig);
-    d.W = T2ptr(s.block, o_w);
-    d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
-    d.pairs = (const int2*)T2ptr(s.block, o_pairs);
-    d.terms = (const Term*)T2ptr(s.block, o_terms);
-    d.term_off = (const int*)T2ptr(s.block, o_toff);
-    s.counters = (unsigned long long*)T2ptr(s.block, o_cnt);
-    d.step = s.counters;
-    d.total = s.counters + 1;
-    d.done_ctr = (unsigned int*)(s.counters + 2);
-    d.status = (int*)(s.counters + 3);
-    d.monitors = (s.flags & MMP_F_NO_MONITORS) ? 0 : 1;
-    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)d.poly, s.poly.data(), s.poly.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess && P) e = cudaMemcpyAsync((void*)d.pairs, s.pairs.data(), P * sizeof(int2), cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess && !s.terms.empty()) e = cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
-    b->Mmax = std::max(b->Mmax, (int)M);
-    b->Pmax = std::max(b->Pmax, (int)(b->raman ? P : 0));
-  }
-  if (build_rc == MMP_OK) {
-    e = cudaMalloc(&b->d_descs, n * sizeof(SolveDesc));
-    if (e != cudaSuccess) build_rc = fail(MMP_ENOMEM, cudaGetErrorString(e));
-  }
-  if (build_rc == MMP_OK) build_rc = upload_desc(b);
-  // Raman spectrum: H = FFT(h_R) * dt * T0 * fR / NT  (src/MultimodePropagation_CPU.cpp:170-176, :241-251)
-  for (uint32_t i = 0; i < n && build_rc == MMP_OK && b->raman; ++i) {
-    Member& s = b->members[i];
+  const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
+  size_t off = 0;
+  off = align_up(off + M * nt * sizeof(double2));                               // psi_hat
+  off = align_up(off + M * nt * sizeof(double2));                               // io
+  off = align_up(off + S * M * nt * t2);                                        // Nh
+  off = align_up(off + M * nt * t2);                                            // U
+  off = align_up(off + M * nt * t2);                                            // sigma
+  off = align_up(off + (b->raman ? P : 0) * nt * t2);                           // W (R)
+  off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));    // H
+  off = align_up(off + s.poly.size() * sizeof(double));
+  off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
+  off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
+  off = align_up(off + (M + 1) * sizeof(int));
+  off = align_up(off + 4 * sizeof(unsigned long long));
+  return off;
+}
+
+// Host setup, device state and uploads for slot idx from params p; leaves the solve
+// at z = 0 with its initial fields transformed. One cudaMalloc for all of it.
+int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
+  Member& s = b->members[idx];
+  s = Member();
+  host_setup(p, s);
+  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+  const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
+  // one allocation: psi_hat | io | Nh | U | sigma | W | H | poly | pairs | terms | term_off | counters
+  size_t off = 0;
+  const size_t o_psi = off; off = align_up(off + M * nt * sizeof(double2));
+  const size_t o_io = off; off = align_up(off + M * nt * sizeof(double2));
+  const size_t o_nh = off; off = align_up(off + S * M * nt * t2);
+  const size_t o_u = off; off = align_up(off + M * nt * t2);
+  const size_t o_sig = off; off = align_up(off + M * nt * t2);
+  const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
+  const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
+  const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
+  const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
+  const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
+  const size_t o_toff = off; off = align_up(off + (M + 1) * sizeof(int));
+  const size_t o_cnt = off; off = align_up(off + 4 * sizeof(unsigned long long));
+  cudaError_t e = cudaMalloc(&s.block, off);
+  if (e != cudaSuccess) return fail(MMP_ENOMEM, "cudaMalloc solver state: " + std::string(cudaGetErrorString(e)));
+  s.bytes = off;
+  CUDA_TRY(cudaMemsetAsync(s.block, 0, off, b->stream));
+  SolveDesc& d = s.desc;
+  std::memset(&d, 0, sizeof(d));
+  d.M = (int)M;
+  d.P = (int)P;
+  d.n_beta = (int)s.n_beta;
+  d.raman = b->raman ? 1 : 0;
+  d.alpha_scale = 2 * M_PI / s.t_final;
+  d.dz = s.delta_z;
+  d.sgn_gamma = s.sgn_gamma;
+  d.one_minus_fR = b->raman ? (1.0 - s.fR) : 1.0;
+  d.inv_nt = 1.0 / (double)nt;
+  d.result_scale = 1.0 / ((double)nt * s.cf);
+  d.energy_scale = s.delta_t * s.T0 / (s.cf * s.cf * (double)nt);
+  d.omega0_T0 = s.omega0 * s.T0;
+  d.photon_scale = d.energy_scale * s.T0 / 1.054571817e-10;
+  d.poly = (const double*)T2ptr(s.block, o_poly);
+  d.psi_hat = (double2*)T2ptr(s.block, o_psi);
+  d.io = (double2*)T2ptr(s.block, o_io);
+  d.Nh = T2ptr(s.block, o_nh);
+  d.U = T2ptr(s.block, o_u);
+  d.sigma = T2ptr(s.block, o_sig);
+  d.W = T2ptr(s.block, o_w);
+  d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
+  d.pairs = (const int2*)T2ptr(s.block, o_pairs);
+  d.terms = (const Term*)T2ptr(s.block, o_terms);
+  d.term_off = (const int*)T2ptr(s.block, o_toff);
+  s.counters = (unsigned long long*)T2ptr(s.block, o_cnt);
+  d.step = s.counters;
+  d.total = s.counters + 1;
+  d.done_ctr = (unsigned int*)(s.counters + 2);
+  d.status = (int*)(s.counters + 3);
+  d.monitors = (s.flags & MMP_F_NO_MONITORS) ? 0 : 1;
+  d.step_limit = ~0ull;
+  CUDA_TRY(cudaMemcpyAsync((void*)d.poly, s.poly.data(), s.poly.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  if (P) CUDA_TRY(cudaMemcpyAsync((void*)d.pairs, s.pairs.data(), P * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+  if (!s.terms.empty())
+    CUDA_TRY(cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  if (b->raman) {
+    // Raman spectrum: H = FFT(h_R) * dt * T0 * fR / NT  (src/MultimodePropagation_CPU.cpp:170-176, :241-251)
     std::vector<double2> hr(nt);
-    for (size_t t = 0; t < nt; ++t) hr[t] = make_double2(params[i]->raman_response[t], 0.0);
-    double2* tmp = s.desc.io;  // staging
-    double2* h64 = (double2*)s.desc.Nh;  // FP64 spectrum scratch (Nh is large enough and unused yet)
-    e = cudaMemcpyAsync(tmp, hr.data(), nt * sizeof(double2), cudaMemcpyHostToDevice, b->stream);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    for (size_t t = 0; t < nt; ++t) hr[t] = make_double2(p->raman_response[t], 0.0);
+    double2* tmp = d.io;                 // staging
+    double2* h64 = (double2*)d.Nh;       // FP64 spectrum scratch (Nh is large enough and unused yet)
+    CUDA_TRY(cudaMemcpyAsync(tmp, hr.data(), nt * sizeof(double2), cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));  // hr is a host temporary
     DftArgs a;
     std::memset(&a, 0, sizeof(a));
     a.in = tmp;
@@ -849,41 +861,93 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
     a.scale = s.delta_t * s.T0 * s.fR / (double)nt;
     a.tw = b->dev->tw;
     void* args[] = {&a};
-    e = launch(b->ks64.dft_fwd, dim3((unsigned)b->ks64.C, 1, 1), b->ks64.nthr, b->ks64.smem, b->ks64.C, b->stream, args);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    CUDA_TRY(launch(b->ks64.dft_fwd, dim3((unsigned)b->ks64.C, 1, 1), b->ks64.nthr, b->ks64.smem, b->ks64.C, b->stream, args));
     const void* conv = b->fp64 ? (const void*)&k_to_t2<double> : (const void*)&k_to_t2<float>;
     const double2* cin = h64;
-    void* cout_ = (void*)s.desc.H;
+    void* cout_ = (void*)d.H;
     size_t cnt = nt;
     void* cargs[] = {(void*)&cin, &cout_, &cnt};
-    e = launch(conv, dim3(64, 1, 1), 256, 0, 1, b->stream, cargs);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
-    e = cudaMemsetAsync(s.desc.Nh, 0, (size_t)b->tab.s * s.M * nt * t2, b->stream);
-    if (e != cudaSuccess) { build_rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
+    CUDA_TRY(launch(conv, dim3(64, 1, 1), 256, 0, 1, b->stream, cargs));
+    CUDA_TRY(cudaMemsetAsync(d.Nh, 0, S * M * nt * t2, b->stream));
   }
-  for (uint32_t i = 0; i < n && build_rc == MMP_OK; ++i)
-    build_rc = member_set_fields(b, i, params[i]->initial_fields);
-  if (build_rc == MMP_OK) {
-    // contraction tile: the largest power of two <= 256 whose U+W tile fits in 100 KB
-    const int rows = b->Mmax + b->Pmax;
-    int TT = 256;
-    while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
-    while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
-    while (TT > (int)nt) TT >>= 1;
-    b->TT = TT;
-    b->contract_smem = (size_t)rows * TT * t2;
-    // terms follow the tiles in shared memory when they fit (else they are read through L1)
-    size_t max_terms = 0;
-    for (auto& s : b->members) max_terms = std::max(max_terms, s.terms.size());
-    b->stage_terms = b->contract_smem + max_terms * sizeof(Term) <= 200 * 1024 ? 1 : 0;
-    if (b->stage_terms) b->contract_smem += max_terms * sizeof(Term);
-    build_rc = autotune(b);
-    e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) build_rc = fail(MMP_ECUDA, cudaGetErrorString(e));
+  b->active[idx] = 1;
+  int rc = upload_desc(b);
+  if (rc) return rc;
+  return member_set_fields(b, idx, p->initial_fields);
+}
+
+// Launch geometry that depends on the members: largest M and P, contraction tile and
+// its shared memory. Returns true when it changed (captured graphs are then stale).
+bool batch_shape(mmp_batch* b) {
+  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+  int Mmax = 0, Pmax = 0;
+  uint32_t span = 0;
+  size_t max_terms = 0;
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    if (!b->active[i]) continue;
+    const Member& s = b->members[i];
+    span = (uint32_t)i + 1;
+    Mmax = std::max(Mmax, (int)s.M);
+    Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
+    max_terms = std::max(max_terms, s.terms.size());
   }
-  if (build_rc != MMP_OK) {
+  // contraction tile: the largest power of two <= 256 whose U + R tile fits in 100 KB
+  const int rows = std::max(Mmax + Pmax, 1);
+  int TT = 256;
+  while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
+  while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
+  while (TT > (int)b->nt) TT >>= 1;
+  size_t smem = (size_t)rows * TT * t2;
+  // terms follow the tiles in shared memory when they fit (else they are read through L1)
+  const int stage_terms = smem + max_terms * sizeof(Term) <= 200 * 1024 ? 1 : 0;
+  if (stage_terms) smem += max_terms * sizeof(Term);
+  const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
+                       stage_terms != b->stage_terms || span != b->span;
+  b->span = span;
+  b->Mmax = Mmax;
+  b->Pmax = Pmax;
+  b->TT = TT;
+  b->contract_smem = smem;
+  b->stage_terms = stage_terms;
+  if (changed && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = 0;
+  }
+  return changed;
+}
+
+int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
+  if (!out) return fail(MMP_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!params || n == 0) return fail(MMP_EINVAL, "empty batch");
+  for (uint32_t i = 0; i < n; ++i) {
+    std::string why;
+    int rc = validate(params[i], why);
+    if (rc) return fail(rc, "member " + std::to_string(i) + ": " + why);
+  }
+  Tableau tab0;
+  tableau_for(params[0], tab0);
+  mmp_batch* b = new mmp_batch();
+  b->capacity = n;
+  b->members.resize(n);
+  b->active.assign(n, 0);
+  int rc = batch_open(b, params[0], tab0);
+  for (uint32_t i = 1; i < n && rc == MMP_OK; ++i)
+    if (!same_shape(b, params[i]))
+      rc = fail(MMP_EINVAL, "batch members must share nt, precision, raman and the RK tableau");
+  for (uint32_t i = 0; i < n && rc == MMP_OK; ++i) rc = member_init(b, i, params[i]);
+  if (rc == MMP_OK) {
+    batch_shape(b);
+    rc = autotune(b);
+  }
+  if (rc == MMP_OK) {
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) rc = fail(MMP_ECUDA, cudaGetErrorString(e));
+  }
+  if (rc != MMP_OK) {
     mmp_batch_destroy(b);
-    return build_rc;
+    return rc;
   }
   *out = b;
   return MMP_OK;
@@ -995,7 +1059,7 @@ int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t
       if (rc) return rc;
     }
   }
-  const int nsol = (int)b->members.size();
+  const int nsol = (int)b->span;
   int rc = launch_row_kernel(b, b->ks, b->ks.prime, b->Mmax, nsol, 0, b->d_descs);
   if (rc) return rc;
   cudaEvent_t ev[2];
@@ -1206,3 +1270,6 @@ const char* mmp_version(void) { return "mmp_b200 0.1.0 (sm_100a)"; }
 uint64_t mmp_kernel_launch_count(void) { return g_launches.load(); }
 
 }  // extern "C"
+
+// serving loop (mmp_server_*): slot pools built on the batch machinery above
+#include "server.cuh"

@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   __syncthreads();
   const SolveDesc& d = sdesc;
   const int q = blockIdx.x / Gm::C;
-  if (q >= d.P) return;  // uniform over the cluster
+  if (q >= d.P || __ldcg(d.step) >= d.step_limit) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
   const int2 lm = d.pairs[q];
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   __syncthreads();
   const SolveDesc& d = sdesc;
   const int p = blockIdx.x / Gm::C;
-  if (p >= d.M) return;  // uniform over the cluster
+  if (p >= d.M || __ldcg(d.step) >= d.step_limit) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
   load_poly(poly, d, p);
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   V* sU = reinterpret_cast<V*>(smem_raw);
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TT;
-  if (t0 >= nt) return;
+  if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;  // empty slot / finished
   const int M = d.M;
   const int raman = d.raman;
   const int P = raman ? d.P : 0;

@@ -82,3 +82,12 @@ def test_validate_rejects_bad_coupling():
 def test_create_without_device_fails_loudly():
     with pytest.raises(mmp.MMPError):
         mmp.Solver(W.small_case())
+    with pytest.raises(mmp.MMPError):
+        mmp.Server()
+
+
+def test_server_structs_match_header():
+    # field order and sizes of the two serving structs as include/mmp.h lays them out
+    assert C.sizeof(capi.mmp_server_config) == 24
+    assert C.sizeof(capi.mmp_request_info) == 48
+    assert [f for f, _ in capi.mmp_request_info._fields_][:4] == ["status", "n_modes", "nt", "steps"]
