@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=6, help="RK steps per process in the CPU sample")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
+    ap.add_argument("--workload", choices=("grin6", "serve"), default="grin6",
+                    help="grin6: the batched 6-mode step (default); serve: the mixed request stream")
+    ap.add_argument("--requests", type=int, default=512, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: mean Poisson arrival rate (1/s)")
+    ap.add_argument("--check", type=int, default=4, help="serve: requests re-solved in FP64 for relL2")
     return ap.parse_args()
 
 
@@ -385,6 +390,95 @@ def ours_arm(args, dist):
     return line
 
 
+def serve_arm(args, dist):
+    """The mixed request stream through the serving loop (mmp_server_*): requests are
+    submitted at their Poisson arrival times from host memory and waited for; the
+    value is the stream's total M*NT*n_steps over the makespan (first arrival to last
+    result, the server's clock), latency = result time - arrival time."""
+    import threading
+    import numpy as np
+    import mm_propagation_b200 as mmp
+    from mm_propagation_b200 import capi, workloads as W
+
+    lib = mmp.lib()
+    stream = W.stream(seed=1000 + dist.rank, n=args.requests, rate_hz=args.rate)
+    handles = [p.to_params() for _, p in stream]          # host-side conversion, before timing
+    work = sum(p.n_modes * p.nt * p.n_steps for _, p in stream)
+    h2d = sum(p.n_modes * p.nt * 16 for _, p in stream)
+    sv = mmp.Server()
+    # warm-up: one short request per kernel shape (first-use costs: tables, graph capture)
+    shapes = {}
+    for _, p in stream:
+        shapes.setdefault((p.nt, p.method_order), p)
+    nw = max(args.warmup, 3)  # same step length, nw steps
+    warm = [sv.submit(p.replace(n_steps=nw, fiber_length=p.fiber_length * nw / p.n_steps))
+            for p in shapes.values()]
+    for rid in warm:
+        sv.wait(rid, timeout=600)
+    ids = [None] * len(stream)
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    clocks.start()
+    l0 = lib.mmp_kernel_launch_count()
+
+    def submitter():
+        t0 = time.perf_counter()
+        for i, (arr, p) in enumerate(stream):
+            dt = arr - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids[i] = sv.submit(p, params=handles[i])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    infos, outs = [None] * len(stream), {}
+    # a seeded sample of requests, re-solved in FP64 after the stream for relL2
+    check = set(np.random.default_rng(7).choice(len(stream), size=min(args.check, len(stream)),
+                                                replace=False).tolist())
+    for i in range(len(stream)):
+        while ids[i] is None:
+            time.sleep(0.001)
+        out, infos[i] = sv.wait(ids[i], timeout=3600)
+        if i in check:
+            outs[i] = out
+    th.join()
+    launches = lib.mmp_kernel_launch_count() - l0
+    clk = clocks.stop()
+    sv.close()
+    first = min(x["submit_s"] for x in infos)
+    last = max(x["done_s"] for x in infos)
+    makespan = dist.max(last - first)
+    value = dist.world * work / makespan
+    lat = np.array([x["done_s"] - x["submit_s"] for x in infos])
+    acc = None
+    if dist.rank == 0 and not args.no_accuracy:
+        errs = []
+        for i in check:
+            p = stream[i][1]
+            with mmp.Solver(p.replace(flags=capi.MMP_F_FP64)) as s:
+                s.propagate(p.n_steps)
+                ref = s.result()
+            errs.append(float(np.sqrt((np.abs(outs[i] - ref) ** 2).sum(-1) / (np.abs(ref) ** 2).sum(-1)).max()))
+        acc = {"relL2_max_served_fp32_vs_fp64": max(errs), "checked_requests": len(check),
+               "tolerance": 1e-5}
+    shapes_n = len({(p.nt, p.method_order) for _, p in stream})
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": 1,
+        "warmup": len(warm), "ms_per_step": 1000.0 * makespan, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"serve: {args.requests} requests, Poisson arrivals at {args.rate}/s, "
+                               "M in {1,3,6,10}, NT 2^11..2^15, L U(0.05,2) m, n_steps U(500,8000), "
+                               "order 4/6, GRIN Q, Raman on (workloads.stream)",
+                   "kernel_shapes": shapes_n, "total_mode_samples_steps": work,
+                   "parallelism": f"replicas x{dist.world}", "l2": "inputs larger than L2"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "mean": float(lat.mean()), "max": float(lat.max())},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+                "note": "one step = the whole stream: submit from host memory, propagate, result to host"},
+        "gpu_launches": int(launches), "clocks": clk, "accuracy": acc,
+    }
+
+
 def batch_tableau(order):
     """Tableau coefficients from the library (mmp_tableau) for the byte model."""
     import mm_propagation_b200 as mmp
@@ -397,7 +491,12 @@ def main():
     args = parse()
     dist = Dist()
     try:
-        line = reference_arm(args, dist) if args.impl == "reference" else ours_arm(args, dist)
+        if args.impl == "reference":
+            line = reference_arm(args, dist)
+        elif args.workload == "serve":
+            line = serve_arm(args, dist)
+        else:
+            line = ours_arm(args, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -217,8 +217,9 @@ class Server:
         _check(lib().mmp_server_create(C.byref(cfg), C.byref(self._ptr)), "mmp_server_create")
         self._shape = {}
 
-    def submit(self, prob) -> int:
-        h = prob.to_params()
+    def submit(self, prob, params=None) -> int:
+        """Queue `prob`; `params` may be its prebuilt prob.to_params() handle."""
+        h = params if params is not None else prob.to_params()
         rid = C.c_uint64(0)
         _check(lib().mmp_server_submit(self._ptr, h.ptr(), C.byref(rid)), "mmp_server_submit")
         self._shape[rid.value] = (prob.n_modes, prob.nt)

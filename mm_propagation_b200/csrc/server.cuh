@@ -2,19 +2,22 @@
 // end of solver.cu: it builds on the batch machinery there (slot pools are batches
 // whose slots are filled and emptied between graph replays).
 //
-// One worker thread owns the device:
-//   1. admit  — scan the waiting requests in submission order; a request joins a pool
-//               of its kernel shape (nt, precision, Raman, tableau) with a free slot, or
-//               a new pool, if its device footprint fits the memory budget (first fit:
-//               a large request that does not fit yet does not block smaller ones).
-//               Admission allocates the solve's state, uploads it, transforms the
-//               initial field, sets the solve's device step limit to its n_steps and
-//               computes U for its first stage.
-//   2. tick   — every pool with solves replays its captured steps_per_tick-step graph
-//               on its own stream (pools overlap on the device); solves whose step
-//               counter reached their limit are skipped by the kernels.
-//   3. retire — finished solves are transformed back (getResult) into host memory,
-//               their state is freed and their slot emptied; waiters are notified.
+// One worker thread owns the device and never waits for the device as a whole; every
+// pool (a batch of solves of one kernel shape: nt, precision, Raman, tableau) runs on
+// its own stream and progresses at its own pace:
+//   * complete — a pool whose last replay finished (its event has fired) credits its
+//                solves with steps_per_tick steps; finished solves are transformed back
+//                (getResult) into host memory, their state returns to the stream-ordered
+//                memory pool and their slot is emptied; waiters are notified.
+//   * admit    — waiting requests, in submission order, join an idle pool of their shape
+//                with a free slot (or a new pool) if their device footprint fits the
+//                memory budget (first fit: a request that does not fit yet does not block
+//                smaller ones behind it). Admission allocates and uploads the solve's
+//                state, transforms its initial field, sets its device step limit to its
+//                n_steps and computes U for its first stage.
+//   * launch   — every idle pool with solves replays its captured steps_per_tick-step
+//                graph and records an event. Solves whose step counter reached their
+//                limit are skipped by the kernels until they are retired.
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -36,7 +39,7 @@ struct Request {
   uint64_t steps = 0;
   double t_submit = 0, t_start = -1, t_done = -1;
   std::vector<double> result;
-  // placement while running
+  // placement while running (worker thread only)
   int pool = -1;
   uint32_t slot = 0;
   uint64_t steps_run = 0;
@@ -47,6 +50,8 @@ struct Pool {
   mmp_batch* b = nullptr;
   std::vector<Request*> slot_req;  // request in each slot (nullptr = free)
   int used = 0;
+  cudaEvent_t done_ev = nullptr;   // recorded after each replay
+  bool in_flight = false;
 };
 
 }  // namespace
@@ -62,6 +67,7 @@ struct mmp_server {
   std::deque<Request*> waiting;
   std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
   std::vector<Pool> pools;
+  cudaMemPool_t mempool = nullptr;
   uint64_t used_bytes = 0;
   std::chrono::steady_clock::time_point t0;
   int fatal = MMP_OK;  // a CUDA error the worker could not recover from
@@ -72,8 +78,6 @@ struct mmp_server {
 
 namespace {
 
-bool pool_matches(const Pool& pl, const mmp_params* p) { return pl.b && same_shape(pl.b, p); }
-
 // Create an empty pool (no solves yet) for the shape of p.
 int pool_open(mmp_server* sv, const mmp_params* p, int* index) {
   Tableau tab;
@@ -82,13 +86,18 @@ int pool_open(mmp_server* sv, const mmp_params* p, int* index) {
   b->capacity = sv->cfg.max_slots;
   b->members.resize(b->capacity);
   b->active.assign(b->capacity, 0);
+  b->mempool = sv->mempool;
   int rc = batch_open(b, p, tab);
   if (rc == MMP_OK) rc = upload_desc(b);
+  Pool pl;
+  if (rc == MMP_OK) {
+    cudaError_t e = cudaEventCreateWithFlags(&pl.done_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = fail(MMP_ECUDA, cudaGetErrorString(e));
+  }
   if (rc) {
     mmp_batch_destroy(b);
     return rc;
   }
-  Pool pl;
   pl.b = b;
   pl.slot_req.assign(b->capacity, nullptr);
   sv->pools.push_back(pl);
@@ -97,24 +106,46 @@ int pool_open(mmp_server* sv, const mmp_params* p, int* index) {
 }
 
 // Device bytes the request will hold (state block), from the host setup alone.
-size_t footprint(const mmp_batch* shape_of, const mmp_params* p) {
+size_t footprint(const mmp_params* p) {
+  mmp_batch shape;
+  shape.fp64 = (p->flags & MMP_F_FP64) != 0;
+  shape.raman = p->raman != 0;
+  shape.nt = p->nt;
+  tableau_for(p, shape.tab);
   Member m;
   host_setup(p, m);
-  return member_bytes(shape_of, m);
+  return member_bytes(&shape, m);
+}
+
+// Empty slot `slot` of pool `pl`: state back to the memory pool (stream-ordered).
+void clear_slot(Pool& pl, uint32_t slot) {
+  mmp_batch* b = pl.b;
+  Member& s = b->members[slot];
+  if (s.block) cudaFreeAsync(s.block, b->stream);
+  if (s.energy) cudaFree(s.energy);
+  s = Member();
+  b->active[slot] = 0;
+  upload_desc(b);
+  batch_shape(b);
 }
 
 int admit(mmp_server* sv, Request* r, int pi, uint32_t slot) {
   Pool& pl = sv->pools[pi];
   mmp_batch* b = pl.b;
   int rc = member_init(b, slot, &r->p);
-  if (rc) return rc;
   Member& s = b->members[slot];
-  s.desc.step_limit = r->p.n_steps;  // this solve stops at its own step count
-  rc = upload_desc(b);
-  if (rc) return rc;
-  batch_shape(b);
-  rc = launch_row_kernel(b, b->ks, b->ks.prime, (int)s.M, 1, 0, b->d_descs + slot);
-  if (rc) return rc;
+  if (rc == MMP_OK) {
+    s.desc.step_limit = r->p.n_steps;  // this solve stops at its own step count
+    rc = upload_desc(b);
+  }
+  if (rc == MMP_OK) {
+    batch_shape(b);
+    rc = launch_row_kernel(b, b->ks, b->ks.prime, (int)s.M, 1, 0, b->d_descs + slot);
+  }
+  if (rc) {
+    if (s.block || b->active[slot]) clear_slot(pl, slot);
+    return rc;
+  }
   pl.slot_req[slot] = r;
   pl.used += 1;
   r->pool = pi;
@@ -125,140 +156,146 @@ int admit(mmp_server* sv, Request* r, int pi, uint32_t slot) {
   return MMP_OK;
 }
 
-void release(mmp_server* sv, Request* r) {
-  Pool& pl = sv->pools[r->pool];
-  mmp_batch* b = pl.b;
-  Member& s = b->members[r->slot];
-  if (s.block) cudaFree(s.block);
-  if (s.energy) cudaFree(s.energy);
-  s = Member();
-  b->active[r->slot] = 0;
-  upload_desc(b);
-  batch_shape(b);
-  pl.slot_req[r->slot] = nullptr;
-  pl.used -= 1;
-  sv->used_bytes -= r->bytes;
-}
-
-void finish(mmp_server* sv, Request* r, int status) {
+void finish(mmp_server* sv, Request* r, int status, std::vector<double>* result) {
   std::lock_guard<std::mutex> lk(sv->mu);
+  if (result) r->result.swap(*result);
+  r->steps = r->steps_run;
   r->status = status;
   r->done = true;
   r->t_done = sv->now();
   sv->cv_done.notify_all();
 }
 
+// A pool's replay finished: credit its solves, retire the finished ones.
+void complete(mmp_server* sv, int pi, int K) {
+  Pool& pl = sv->pools[pi];
+  pl.in_flight = false;
+  for (uint32_t slot = 0; slot < pl.b->capacity; ++slot) {
+    Request* r = pl.slot_req[slot];
+    if (!r) continue;
+    r->steps_run = std::min<uint64_t>(r->steps_run + K, r->p.n_steps);
+    if (r->steps_run < r->p.n_steps && sv->fatal == MMP_OK) continue;
+    const Member& s = pl.b->members[slot];
+    int status = sv->fatal;
+    if (status == MMP_OK) {
+      int st = 0;
+      cudaError_t e = cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
+                                 cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) status = fail(MMP_ECUDA, cudaGetErrorString(e));
+      else if (st & kStatusTimeout) status = MMP_ETIMEOUT;
+      else if (st & kStatusNonFinite) status = MMP_ENONFINITE;
+    }
+    std::vector<double> out((size_t)2 * r->p.n_modes * r->p.nt);
+    if (status == MMP_OK) status = member_result(pl.b, slot, out.data());
+    clear_slot(pl, slot);
+    pl.slot_req[slot] = nullptr;
+    pl.used -= 1;
+    sv->used_bytes -= r->bytes;
+    finish(sv, r, status, status == MMP_OK ? &out : nullptr);
+  }
+}
+
+// Admit what fits from the waiting list. Returns true if anything was admitted or failed.
+bool admit_waiting(mmp_server* sv) {
+  std::vector<Request*> snapshot;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    snapshot.assign(sv->waiting.begin(), sv->waiting.end());
+  }
+  bool changed = false;
+  for (Request* r : snapshot) {
+    int rc = sv->fatal;  // after a device failure every waiting request fails with it
+    int pi = -1;
+    bool deferred = false;
+    if (rc == MMP_OK) {
+      for (size_t i = 0; i < sv->pools.size(); ++i) {
+        Pool& pl = sv->pools[i];
+        if (pl.used >= (int)pl.b->capacity || !same_shape(pl.b, &r->p)) continue;
+        if (pl.in_flight) {
+          deferred = true;  // a pool with room is busy: try again after its replay
+          continue;
+        }
+        pi = (int)i;
+        break;
+      }
+      if (pi < 0 && deferred) continue;
+      const size_t need = footprint(&r->p);
+      if (sv->used_bytes + need > sv->cfg.memory_budget) {
+        if (sv->used_bytes != 0) continue;  // first fit: try the next waiting request
+        rc = fail(MMP_ENOMEM, "request larger than the server's memory budget");
+      }
+      if (rc == MMP_OK && pi < 0) rc = pool_open(sv, &r->p, &pi);
+    }
+    if (rc == MMP_OK) {
+      uint32_t slot = 0;
+      while (sv->pools[pi].slot_req[slot]) ++slot;
+      rc = admit(sv, r, pi, slot);
+    }
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      auto it = std::find(sv->waiting.begin(), sv->waiting.end(), r);
+      if (it != sv->waiting.end()) sv->waiting.erase(it);
+    }
+    if (rc) finish(sv, r, rc, nullptr);
+    changed = true;
+  }
+  return changed;
+}
+
 void worker_loop(mmp_server* sv) {
   cudaSetDevice(sv->device);
   const int K = (int)sv->cfg.steps_per_tick;
   while (true) {
-    // ---- admit
-    std::vector<Request*> batch_in;
+    bool progressed = false, any_in_flight = false;
+    // complete
+    for (size_t pi = 0; pi < sv->pools.size(); ++pi) {
+      Pool& pl = sv->pools[pi];
+      if (!pl.in_flight) continue;
+      cudaError_t e = cudaEventQuery(pl.done_ev);
+      if (e == cudaErrorNotReady) {
+        any_in_flight = true;
+        continue;
+      }
+      if (e != cudaSuccess && sv->fatal == MMP_OK) sv->fatal = fail(MMP_ECUDA, cudaGetErrorString(e));
+      complete(sv, (int)pi, K);
+      progressed = true;
+    }
+    // admit
     {
       std::unique_lock<std::mutex> lk(sv->mu);
-      bool any_active = false;
-      for (auto& pl : sv->pools) any_active |= pl.used > 0;
-      if (!any_active && sv->waiting.empty() && !sv->stop)
-        sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
       if (sv->stop) break;
-      batch_in.assign(sv->waiting.begin(), sv->waiting.end());
-    }
-    for (Request* r : batch_in) {
-      int rc = sv->fatal;  // after a device failure every waiting request fails with it
-      int pi = -1;
-      for (size_t i = 0; rc == MMP_OK && i < sv->pools.size(); ++i)
-        if (pool_matches(sv->pools[i], &r->p) && sv->pools[i].used < (int)sv->pools[i].b->capacity) {
-          pi = (int)i;
-          break;
-        }
-      if (rc == MMP_OK && pi < 0) rc = pool_open(sv, &r->p, &pi);
-      if (rc == MMP_OK) {
-        const size_t need = footprint(sv->pools[pi].b, &r->p);
-        if (sv->used_bytes + need > sv->cfg.memory_budget) {
-          if (sv->used_bytes != 0) continue;  // first fit: try the next waiting request
-          rc = fail(MMP_ENOMEM, "request larger than the server's memory budget");
-        }
-      }
-      uint32_t slot = 0;
-      bool attempted = false;
-      if (rc == MMP_OK) {
-        while (sv->pools[pi].slot_req[slot]) ++slot;
-        attempted = true;
-        rc = admit(sv, r, pi, slot);
-      }
-      {
-        std::lock_guard<std::mutex> lk(sv->mu);
-        auto it = std::find(sv->waiting.begin(), sv->waiting.end(), r);
-        if (it != sv->waiting.end()) sv->waiting.erase(it);
-      }
-      if (rc) {
-        Pool* pl = attempted ? &sv->pools[pi] : nullptr;
-        if (pl && pl->b->members[slot].block && !pl->slot_req[slot]) {  // partly admitted: undo
-          Member& s = pl->b->members[slot];
-          cudaFree(s.block);
-          if (s.energy) cudaFree(s.energy);
-          s = Member();
-          pl->b->active[slot] = 0;
-          upload_desc(pl->b);
-          batch_shape(pl->b);
-        }
-        finish(sv, r, rc);
+      bool any_used = false;
+      for (auto& pl : sv->pools) any_used |= pl.used > 0;
+      if (!any_used && sv->waiting.empty()) {
+        sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+        continue;
       }
     }
-    // ---- tick: one graph replay per pool with solves, pools on their own streams
-    bool ran = false;
+    progressed |= admit_waiting(sv);
+    // launch
     for (auto& pl : sv->pools) {
-      if (pl.used == 0) continue;
+      if (pl.in_flight || pl.used == 0) continue;
       mmp_batch* b = pl.b;
       int rc = build_graph(b, K);
       if (rc == MMP_OK) {
         cudaError_t e = cudaGraphLaunch(b->graph, b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(pl.done_ev, b->stream);
         if (e != cudaSuccess) rc = fail(MMP_ECUDA, cudaGetErrorString(e));
         else g_launches.fetch_add((uint64_t)K * b->kernels_per_step, std::memory_order_relaxed);
       }
-      if (rc) {
-        sv->fatal = rc;
-      }
-      ran = true;
+      if (rc && sv->fatal == MMP_OK) sv->fatal = rc;
+      if (rc) cudaEventRecord(pl.done_ev, b->stream);  // completes at once; solves fail there
+      pl.in_flight = true;
+      any_in_flight = true;
+      progressed = true;
     }
-    if (!ran) continue;
-    // ---- retire
-    for (size_t pi = 0; pi < sv->pools.size(); ++pi) {
-      Pool& pl = sv->pools[pi];
-      if (pl.used == 0) continue;
-      cudaError_t e = cudaStreamSynchronize(pl.b->stream);
-      if (e != cudaSuccess && sv->fatal == MMP_OK) sv->fatal = fail(MMP_ECUDA, cudaGetErrorString(e));
-      for (uint32_t slot = 0; slot < pl.b->capacity; ++slot) {
-        Request* r = pl.slot_req[slot];
-        if (!r) continue;
-        r->steps_run = std::min<uint64_t>(r->steps_run + K, r->p.n_steps);
-        if (r->steps_run < r->p.n_steps && sv->fatal == MMP_OK) continue;
-        // finished (or the device failed): status bits, then the result
-        const Member& s = pl.b->members[slot];
-        int st = 0;
-        int status = sv->fatal;
-        if (status == MMP_OK) {
-          cudaError_t e = cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
-                                     cudaMemcpyDeviceToHost);
-          if (e != cudaSuccess) status = fail(MMP_ECUDA, cudaGetErrorString(e));
-          else if (st & kStatusTimeout) status = MMP_ETIMEOUT;
-          else if (st & kStatusNonFinite) status = MMP_ENONFINITE;
-        }
-        std::vector<double> out((size_t)2 * r->p.n_modes * r->p.nt);
-        if (status == MMP_OK) status = member_result(pl.b, slot, out.data());
-        {
-          std::lock_guard<std::mutex> lk(sv->mu);
-          r->result.swap(out);
-          r->steps = r->steps_run;
-        }
-        release(sv, r);
-        finish(sv, r, status);
-      }
-    }
+    if (!progressed && any_in_flight) std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
+  for (auto& pl : sv->pools)
+    if (pl.in_flight) cudaEventSynchronize(pl.done_ev);
 }
 
-int copy_request(const mmp_params* p, Request* r) {
+void copy_request(const mmp_params* p, Request* r) {
   r->p = *p;
   r->beta.assign(p->dispersion, p->dispersion + (size_t)p->n_modes * p->n_beta);
   r->nz.assign(p->coupling, p->coupling + p->n_nonzeros);
@@ -269,7 +306,6 @@ int copy_request(const mmp_params* p, Request* r) {
   r->p.initial_fields = r->fields.data();
   r->p.raman_response = r->raman.empty() ? nullptr : r->raman.data();
   r->p.flags |= MMP_F_NO_MONITORS;  // served solves keep no per-step monitors
-  return MMP_OK;
 }
 
 }  // namespace
@@ -279,29 +315,32 @@ extern "C" {
 int mmp_server_create(const mmp_server_config* cfg, mmp_server** out) {
   if (!out) return fail(MMP_EINVAL, "out is NULL");
   *out = nullptr;
-  mmp_server* sv = new mmp_server();
+  std::unique_ptr<mmp_server> sv(new mmp_server());
   if (cfg) sv->cfg = *cfg;
   if (!sv->cfg.max_slots) sv->cfg.max_slots = 64;
   if (!sv->cfg.steps_per_tick) sv->cfg.steps_per_tick = 32;
-  cudaError_t e = cudaGetDevice(&sv->device);
-  if (e != cudaSuccess) {
-    delete sv;
-    return fail(MMP_ECUDA, cudaGetErrorString(e));
-  }
+  CUDA_TRY(cudaGetDevice(&sv->device));
   DeviceRes* res = nullptr;
   int rc = ensure_device(sv->device, &res);
-  if (rc) {
-    delete sv;
-    return rc;
-  }
+  if (rc) return rc;
   if (!sv->cfg.memory_budget) {
     size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
+    CUDA_TRY(cudaMemGetInfo(&fr, &tot));
     sv->cfg.memory_budget = (uint64_t)(0.8 * (double)fr);
   }
+  // the server's own stream-ordered pool; freed blocks stay reserved for reuse
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = sv->device;
+  CUDA_TRY(cudaMemPoolCreate(&sv->mempool, &props));
+  uint64_t keep = ~0ull;
+  CUDA_TRY(cudaMemPoolSetAttribute(sv->mempool, cudaMemPoolAttrReleaseThreshold, &keep));
   sv->t0 = std::chrono::steady_clock::now();
-  sv->worker = std::thread(worker_loop, sv);
-  *out = sv;
+  mmp_server* raw = sv.release();
+  raw->worker = std::thread(worker_loop, raw);
+  *out = raw;
   return MMP_OK;
 }
 
@@ -369,7 +408,11 @@ void mmp_server_destroy(mmp_server* sv) {
   }
   if (sv->worker.joinable()) sv->worker.join();
   cudaSetDevice(sv->device);
-  for (auto& pl : sv->pools) mmp_batch_destroy(pl.b);
+  for (auto& pl : sv->pools) {
+    if (pl.done_ev) cudaEventDestroy(pl.done_ev);
+    mmp_batch_destroy(pl.b);
+  }
+  if (sv->mempool) cudaMemPoolDestroy(sv->mempool);
   delete sv;
 }
 

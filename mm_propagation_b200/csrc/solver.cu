@@ -444,6 +444,9 @@ struct mmp_batch {
   std::vector<uint8_t> active;
   SolveDesc* d_descs = nullptr;
   uint32_t span = 0;  // slots the kernels are launched over: highest active slot + 1
+  // Served pools take solve state from a stream-ordered pool (no device-wide
+  // synchronisation when a solve is admitted or retired); null: cudaMalloc/cudaFree.
+  cudaMemPool_t mempool = nullptr;
   int Mmax = 0, Pmax = 0;
   int TT = 32;
   int stage_terms = 0;
@@ -803,8 +806,12 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
   const size_t o_toff = off; off = align_up(off + (M + 1) * sizeof(int));
   const size_t o_cnt = off; off = align_up(off + 4 * sizeof(unsigned long long));
-  cudaError_t e = cudaMalloc(&s.block, off);
-  if (e != cudaSuccess) return fail(MMP_ENOMEM, "cudaMalloc solver state: " + std::string(cudaGetErrorString(e)));
+  cudaError_t e = b->mempool ? cudaMallocFromPoolAsync(&s.block, off, b->mempool, b->stream)
+                             : cudaMalloc(&s.block, off);
+  if (e != cudaSuccess) {
+    s.block = nullptr;
+    return fail(MMP_ENOMEM, "allocating solver state: " + std::string(cudaGetErrorString(e)));
+  }
   s.bytes = off;
   CUDA_TRY(cudaMemsetAsync(s.block, 0, off, b->stream));
   SolveDesc& d = s.desc;
@@ -1103,9 +1110,10 @@ void mmp_batch_destroy(mmp_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (auto& s : b->members) {
-    if (s.block) cudaFree(s.block);
+    if (s.block) b->mempool ? cudaFreeAsync(s.block, b->stream) : cudaFree(s.block);
     if (s.energy) cudaFree(s.energy);
   }
+  if (b->mempool && b->stream) cudaStreamSynchronize(b->stream);
   if (b->d_descs) cudaFree(b->d_descs);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

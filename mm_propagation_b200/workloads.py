@@ -365,6 +365,56 @@ def sweep28(seed: int = 0, index: int = 0, batch: int = 32, nt: int = 65536,
         notes={"index": index, "batch": batch, "peak_total_w": float(pk)})
 
 
+STREAM_PHASE_CAP = 5.6e-3  # nonlinear_phase_per_step of grin6 at 10 W total peak
+STREAM_TOTAL_PHASE_CAP = 5000 * STREAM_PHASE_CAP  # ... over its 5000 steps
+
+
+def stream(seed: int = 0, n: int = 512, rate_hz: float = 200.0, median_peak_w: float = 2e4,
+           peak_sigma: float = 0.5, phase_cap: float = STREAM_PHASE_CAP,
+           total_phase_cap: float = STREAM_TOTAL_PHASE_CAP, flags: int = 0):
+    """The served mixed stream: n requests with Poisson arrivals (mean rate_hz);
+    each draws M from {1,3,6,10}, NT from {2^11..2^15}, fiber length U(0.05, 2) m,
+    n_steps U(500, 8000), order 4 or 6, GRIN-pattern Q (about 60 (M/6)^2 non-zeros,
+    lognormal around 5e12), Raman on, a 20 ps window, grin6's beta distributions
+    and a 0.2 ps Gaussian split by Dirichlet(1) fractions with total peak power
+    lognormal(median_peak_w, peak_sigma). Each request's power is then lowered, where
+    needed, until its nonlinear phase per step is at most `phase_cap` and over the
+    whole fiber at most `total_phase_cap` (the levels of the 6-mode workload at 10 W,
+    where it is converged and FP32 bulk meets relL2 <= 1e-5): at the drawn kilowatt
+    powers RK4/RK6 with these step lengths diverge. Returns [(arrival_s, Problem)]
+    sorted by arrival."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, size=n))
+    window, fwhm = 20.0, 0.2
+    out = []
+    for i in range(n):
+        M = int(rng.choice([1, 3, 6, 10]))
+        nt = int(2 ** rng.integers(11, 16))
+        L = float(rng.uniform(0.05, 2.0))
+        steps = int(rng.integers(500, 8001))
+        order = int(rng.choice([4, 6]))
+        drawn = float(median_peak_w * math.exp(peak_sigma * rng.standard_normal()))
+        beta = np.zeros((M, 3))
+        beta[:, 1] = rng.uniform(-2e-3, 2e-3, size=M)
+        beta[:, 2] = rng.uniform(0.015, 0.025, size=M)
+        Q = grin_coupling(M, max(1, round(60 * (M / 6) ** 2)), rng)
+        frac = rng.dirichlet(np.ones(M))
+        phases = rng.uniform(0, 2 * math.pi, size=M)
+        unit = np.stack([gaussian(nt, window, fwhm, frac[p], phases[p]) for p in range(M)])
+        prob = Problem(
+            n_modes=M, nt=nt, dispersion=beta, coupling=Q, initial_fields=unit,
+            time_window=window, pulse_width=fwhm / (2 * math.sqrt(math.log(2))),
+            fiber_length=L, n_steps=steps, method_order=order,
+            raman_proportion=0.18, raman_response=raman_response(nt, window), raman=True,
+            flags=flags, name="stream", seed=seed)
+        per_w = nonlinear_phase_per_step(prob)  # phase is linear in power
+        peak = min(drawn, phase_cap / per_w, total_phase_cap / (per_w * steps))
+        prob = prob.replace(initial_fields=unit * math.sqrt(peak),
+                            notes={"index": i, "peak_drawn_w": drawn, "peak_total_w": peak})
+        out.append((float(arrivals[i]), prob))
+    return out
+
+
 def small_case(seed: int = 0, M: int = 2, nt: int = 256, n_steps: int = 20, order: int = 4,
                raman: bool = True, window: float = 10.0, fiber_length: float = 0.01,
                peak_w: float = 200.0, nnz_target: int = 12, physical_order: bool = False,
