@@ -156,6 +156,37 @@ int mmp_get_info(mmp_solver* s, mmp_info* info);
 /* ~MultimodePropagation (include/MultimodePropagation.hpp:39). NULL is allowed. */
 void mmp_solver_destroy(mmp_solver* s);
 
+/* ---- chunked propagation and files (the MEX front end, matlab/mm_propagation.cpp, and
+ * the driver, simulations/main.cpp) ---------------------------------------------------- */
+/* The MEX front end's n_save loop (matlab/mm_propagation.cpp:61-91): n_save chunks of
+ * n_steps / n_save RK steps, the last one plus n_steps % n_save; after chunk i the
+ * result is read back into fields[i][M][NT][2] (may be NULL), Z[i] = steps so far *
+ * fiber_length / n_steps in metres (may be NULL), elapsed_s[i] = seconds since the call
+ * began (may be NULL). z_mode 0 carries z across the chunks, so every snapshot is the
+ * field at Z[i]; z_mode 1 restarts z at every chunk as the reference's computeLawsonRK
+ * does (src/MultimodePropagation.cpp:158-163), which is what the MEX front end
+ * saves. The first chunk starts like mmp_propagate (z = 0 unless MMP_F_CONTINUOUS). */
+int mmp_propagate_snapshots(mmp_solver* s, uint32_t n_save, int z_mode, double* fields, double* Z,
+                            double* elapsed_s);
+
+/* The MEX front end's dense coupling input (matlab/mm_propagation.cpp:186-209): q[M^4]
+ * in MATLAB order (p fastest, then k, l, m) to the non-zero list, in the order the
+ * MEX inserts it (which decides the reference's unique_pairs). *n receives the count;
+ * at most cap entries are written to out (out may be NULL to count). */
+int mmp_coupling_from_dense(uint32_t M, const double* q, mmp_nz* out, uint32_t cap, uint32_t* n);
+
+/* The driver's text dump (simulations/main.cpp:101-103): one line per sample i,
+ * |phi0_0[i]| ; ... ; |phi0_{M-1}[i]| ; |phi_0[i]| ; ... ; |phi_{M-1}[i]| in the default
+ * iostream number format (%g). phi0 may be NULL (only the output columns). */
+int mmp_write_abs_text(const char* path, uint32_t M, uint32_t nt, const double* phi0, const double* phi);
+
+/* The struct the MEX front end saves (matlab/mm_propagation.cpp:280-325), as a MATLAB
+ * Level-5 MAT-file (readable by MATLAB's load and scipy.io.loadmat) holding variable
+ * `name` (NULL: "output") = struct with Z (1x1 double, m), fields (M x NT complex double)
+ * and cpu_time (1x1 double, s). phi is [M][NT][2]. */
+int mmp_write_mat(const char* path, const char* name, double Z, uint32_t M, uint32_t nt, const double* phi,
+                  double cpu_time);
+
 /* ---- batches: many independent solves advanced by the same launches -------------- */
 /* All members must share nt, flags & MMP_F_FP64, raman and the RK tableau; n_modes,
  * coupling, dispersion, fields and lengths may differ. Member i is addressed by index. */

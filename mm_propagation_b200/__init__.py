@@ -14,6 +14,7 @@ raise. There is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -99,6 +100,17 @@ class Solver:
     def set_fields(self, phi0: np.ndarray):
         a = np.ascontiguousarray(phi0, dtype=np.complex128)
         _check(lib().mmp_set_fields(self._ptr, _dptr(a.view(np.float64))), "mmp_set_fields")
+
+    def snapshots(self, n_save: int, z_mode: int = 0):
+        """The MEX front end's chunked run (mmp_propagate_snapshots): returns
+        (fields complex128 [n_save][M][NT], Z [n_save] in m, elapsed [n_save] in s).
+        z_mode 0 carries z across chunks; 1 restarts it per chunk as the reference does."""
+        f = np.empty((n_save, self.M, self.nt), dtype=np.complex128)
+        z = np.empty(n_save)
+        t = np.empty(n_save)
+        _check(lib().mmp_propagate_snapshots(self._ptr, int(n_save), int(z_mode), _dptr(f.view(np.float64)),
+                                             _dptr(z), _dptr(t)), "mmp_propagate_snapshots")
+        return f, z, t
 
     def monitors(self, max_steps: int | None = None):
         info = self.info()
@@ -259,6 +271,40 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def coupling_from_dense(q: np.ndarray) -> np.ndarray:
+    """Dense Q[p, k, l, m] (numpy indexing) to the non-zero list in the order the MEX
+    front end inserts it (MATLAB order: p fastest, then k, l, m), as workloads' NZ dtype."""
+    from .workloads import NZ_DTYPE
+    q = np.asarray(q, dtype=np.float64)
+    M = q.shape[0]
+    if q.shape != (M, M, M, M):
+        raise ValueError("dense coupling must be M x M x M x M")
+    flat = np.ascontiguousarray(q.transpose(3, 2, 1, 0)).ravel()   # p fastest in memory
+    n = C.c_uint32(0)
+    _check(lib().mmp_coupling_from_dense(M, _dptr(flat), None, 0, C.byref(n)), "mmp_coupling_from_dense")
+    out = np.zeros(max(n.value, 1), dtype=NZ_DTYPE)   # same layout as mmp_nz
+    _check(lib().mmp_coupling_from_dense(M, _dptr(flat), out.ctypes.data_as(C.POINTER(capi.mmp_nz)),
+                                         n.value, C.byref(n)), "mmp_coupling_from_dense")
+    return out[:n.value]
+
+
+def write_abs_text(path: str, phi: np.ndarray, phi0: np.ndarray | None = None):
+    """The driver's |phi| text dump (mmp_write_abs_text)."""
+    a = np.ascontiguousarray(phi, dtype=np.complex128)
+    b = None if phi0 is None else np.ascontiguousarray(phi0, dtype=np.complex128)
+    M, nt = a.shape
+    _check(lib().mmp_write_abs_text(os.fsencode(path), M, nt, None if b is None else _dptr(b.view(np.float64)),
+                                    _dptr(a.view(np.float64))), "mmp_write_abs_text")
+
+
+def write_mat(path: str, Z: float, fields: np.ndarray, cpu_time: float, name: str = "output"):
+    """The MEX front end's saved struct {Z, fields, cpu_time} as a Level-5 MAT-file."""
+    a = np.ascontiguousarray(fields, dtype=np.complex128)
+    M, nt = a.shape
+    _check(lib().mmp_write_mat(os.fsencode(path), name.encode(), float(Z), M, nt, _dptr(a.view(np.float64)),
+                               float(cpu_time)), "mmp_write_mat")
 
 
 def dft(x: np.ndarray, inverse: bool = False, fp64: bool = True) -> np.ndarray:

@@ -27,6 +27,8 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE] + ARCH
+CXX = os.environ.get("MMP_CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++")
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I", INCLUDE]
 LOGN_RANGE = range(6, 17)
 # row-split variants (kernel_table.h kSplit*): log2 NT ranges per precision
 SPLIT_F32 = range(12, 16)
@@ -66,6 +68,8 @@ def _units():
             continue
         obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
         units.append((src, obj, []))
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cpp"))):  # host-only units
+        units.append((src, os.path.join(BUILD, os.path.basename(src)[:-4] + ".o"), []))
     return units
 
 
@@ -74,8 +78,11 @@ def _compile(unit, force: bool, verbose: bool):
     deps = [src] + _headers() + [os.path.abspath(__file__)]
     if not force and not _stale(obj, deps):
         return obj, False, ""
-    cmd = [nvcc(), "-c", src, "-o", obj] + NVCC_FLAGS + defs
-    if verbose:
+    if src.endswith(".cpp"):
+        cmd = [CXX, "-c", src, "-o", obj] + CXX_FLAGS
+    else:
+        cmd = [nvcc(), "-c", src, "-o", obj] + NVCC_FLAGS + defs
+    if verbose and not src.endswith(".cpp"):
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -125,7 +125,15 @@ SIGNATURES = {
                          C.POINTER(C.c_double)]),
     "mmp_dft_noalloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]),
-    "mmp_server_create": (C.c_int, [C.POINTER(mmp_server_config), C.POINTER(C.c_void_p)]),
+    "mmp_propagate_snapshots": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "mmp_coupling_from_dense": (C.c_int, [C.c_uint32, C.POINTER(C.c_double), C.POINTER(mmp_nz),
+                                          C.c_uint32, C.POINTER(C.c_uint32)]),
+    "mmp_write_abs_text": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]),
+    "mmp_write_mat": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_uint32, C.c_uint32,
+                                C.POINTER(C.c_double), C.c_double]),
+    "mmp_server_create":(C.c_int, [C.POINTER(mmp_server_config), C.POINTER(C.c_void_p)]),
     "mmp_server_submit": (C.c_int, [C.c_void_p, C.POINTER(mmp_params), C.POINTER(C.c_uint64)]),
     "mmp_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
     "mmp_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_double),

@@ -6,6 +6,7 @@
 // everything per step runs on the device in the kernels of stage_kernels.cuh.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -77,7 +78,16 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-#define CUDA_TRY(expr)                                                                   \
+}  // namespace
+
+namespace mmp_detail {
+// for the host-only units (io.cpp): record the text mmp_last_error returns
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace mmp_detail
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                 \
   do {                                                                                   \
     cudaError_t e_ = (expr);                                                             \
     if (e_ != cudaSuccess) {                                                             \
@@ -263,6 +273,7 @@ void tableau_for(const mmp_params* p, Tableau& t) {
 struct Member {
   uint32_t M = 0, nt = 0, n_beta = 0, n_steps = 0;
   double T0 = 0, LD = 0, t_final = 0, delta_t = 0, z_final = 0, delta_z = 0, cf = 0;
+  double fiber_length = 0;  // m (snapshot positions)
   double max_beta2 = 0, max_Q = 0, sgn_gamma = 1, fR = 0, omega0 = 0;
   std::vector<uint32_t> unique_pairs;
   std::vector<int2> pairs;
@@ -358,6 +369,7 @@ void host_setup(const mmp_params* p, Member& s) {
   s.t_final = p->time_window / s.T0;                                   // :47-48
   s.delta_t = s.t_final / s.nt;
   s.z_final = p->fiber_length / s.LD;                                  // :50-51
+  s.fiber_length = p->fiber_length;
   s.delta_z = s.z_final / p->n_steps;
   s.cf = std::sqrt(std::fabs(gamma) * s.LD) * std::sqrt(max_Q);        // :53
   s.fR = p->raman ? p->raman_proportion : 0.0;
@@ -1158,6 +1170,36 @@ int mmp_propagate_default(mmp_solver* s) {
 int mmp_get_result(mmp_solver* s, double* out) {
   if (!s) return fail(MMP_EINVAL, "NULL solver");
   return member_result(s->b, 0, out);
+}
+
+int mmp_propagate_snapshots(mmp_solver* sol, uint32_t n_save, int z_mode, double* fields, double* Z,
+                            double* elapsed_s) {
+  if (!sol) return fail(MMP_EINVAL, "NULL solver");
+  if (n_save == 0) return fail(MMP_EINVAL, "n_save must be >= 1");
+  if (z_mode != 0 && z_mode != 1) return fail(MMP_EINVAL, "z_mode must be 0 (continuous) or 1 (reference)");
+  const auto t0 = std::chrono::steady_clock::now();
+  mmp_batch* b = sol->b;
+  Member& s = b->members[0];
+  // matlab/mm_propagation.cpp:61-91: n_save - 1 chunks of n_steps / n_save steps, then
+  // one of n_steps / n_save + n_steps % n_save; Z += nz * fiber_length / n_steps
+  const uint32_t nz = s.n_steps / n_save;
+  const double delta_Z = s.fiber_length / s.n_steps;
+  const uint32_t flags0 = s.flags;
+  const size_t row = (size_t)2 * s.M * s.nt;
+  double z_acc = 0.0;
+  for (uint32_t i = 0; i < n_save; ++i) {
+    const uint32_t n = (i + 1 < n_save) ? nz : nz + s.n_steps % n_save;
+    if (z_mode == 0 && i > 0) s.flags |= MMP_F_CONTINUOUS;  // later chunks carry z on
+    int rc = batch_propagate_async(b, n);
+    s.flags = flags0;
+    if (rc == MMP_OK) rc = batch_sync(b);
+    if (rc == MMP_OK && fields) rc = member_result(b, 0, fields + i * row);
+    if (rc) return rc;
+    z_acc += n * delta_Z;
+    if (Z) Z[i] = z_acc;
+    if (elapsed_s) elapsed_s[i] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return MMP_OK;
 }
 
 int mmp_set_fields(mmp_solver* s, const double* phi0) {

@@ -262,6 +262,19 @@ class OracleSolver:
                 self.E[i] = self.E[i] * self.E1
             self.z += self.delta_z
 
+    def continue_lawson_rk(self, nz):
+        """nz more steps from the current z, without the reset of initLawsonRK: the
+        stage exponentials are rebuilt at z (E_i = exp(L (z + c_i h))) and the steps run
+        as in computeLawsonRK. What a correct chunked propagation does."""
+        if not hasattr(self, "L"):
+            self._init_lawson()
+        self.E = [np.exp(self.L * (self.z + ci * self.delta_z)) for ci in self.c]
+        for _ in range(nz):
+            self.apply_rk(self.delta_z)
+            for i in range(self.s):
+                self.E[i] = self.E[i] * self.E1
+            self.z += self.delta_z
+
     def get_result(self):
         """getResult (src/MultimodePropagation_CPU.cpp:88-104)."""
         if not hasattr(self, "L"):
@@ -276,6 +289,52 @@ def solve(prob, chunks=None, physical_pairs=False):
     for nz in (chunks if chunks is not None else [prob.n_steps]):
         sol.compute_lawson_rk(nz)
     return sol.get_result()
+
+
+def coupling_from_dense(q):
+    """setCouplingCoefficients (matlab/mm_propagation.cpp:186-209): walk the dense
+    M^4 array in MATLAB element order (p fastest, then k, l, m) and append every
+    non-zero (k, l, m, value) to Q^(p). Returns [(p, k, l, m, value)] in that order."""
+    q = np.asarray(q, dtype=np.float64)
+    M = q.shape[0]
+    out = []
+    for m in range(M):
+        for l in range(M):
+            for k in range(M):
+                for p in range(M):
+                    v = float(q[p, k, l, m])
+                    if v != 0.0:
+                        out.append((p, k, l, m, v))
+    return out
+
+
+def abs_text_lines(phi0, phi):
+    """simulations/main.cpp:101-103: per sample, |phi0_p| then |phi_p| for every mode,
+    joined by " ; ", numbers as the default iostream prints them (%g)."""
+    cols = [np.abs(a) for a in (list(phi0) if phi0 is not None else []) + list(phi)]
+    return [" ; ".join("%g" % c[i] for c in cols) for i in range(len(cols[0]))]
+
+
+def snapshots(prob, n_save, z_mode=0):
+    """The MEX front end's n_save loop (matlab/mm_propagation.cpp:61-91): n_save - 1
+    chunks of n_steps // n_save steps, then one of n_steps // n_save + n_steps % n_save,
+    getResult after each, Z += nz * fiber_length / n_steps. z_mode 1 calls
+    computeLawsonRK per chunk (z restarts at 0 each time, as the reference does);
+    z_mode 0 continues z across chunks. Returns (fields [n_save][M][NT], Z [n_save])."""
+    sol = OracleSolver(prob)
+    nz = prob.n_steps // n_save
+    delta_Z = prob.fiber_length / prob.n_steps
+    out, Z, z_acc = [], [], 0.0
+    for i in range(n_save):
+        n = nz if i < n_save - 1 else nz + prob.n_steps % n_save
+        if z_mode == 1 or i == 0:
+            sol.compute_lawson_rk(n)
+        else:
+            sol.continue_lawson_rk(n)
+        out.append(sol.get_result())
+        z_acc += n * delta_Z
+        Z.append(z_acc)
+    return np.stack(out), np.array(Z)
 
 
 def rel_l2_per_mode(x, ref):

@@ -38,6 +38,24 @@ def test_restatement_matches_reference_live(seed, M, nt, order, raman):
     assert mo.rel_l2_per_mode(mo.solve(prob), ref).max() < 1e-12
 
 
+@needs_ref
+def test_reference_z_snapshots_match_reference_chunked_calls():
+    # the MEX loop with z_mode 1: snapshot i is the reference after i+1 computeLawsonRK calls
+    prob = W.small_case(seed=34, M=3, nt=128, n_steps=11)
+    snaps, Z = mo.snapshots(prob, 3, z_mode=1)
+    chunks = [3, 3, 5]
+    for i in range(3):
+        ref, _ = ref_lib.run(prob, chunks[:i + 1])
+        assert mo.rel_l2_per_mode(snaps[i], ref).max() < 1e-12
+    assert np.allclose(Z, np.cumsum(chunks) * prob.fiber_length / prob.n_steps, rtol=1e-15)
+
+
+def test_continuous_snapshots_end_at_the_single_call_result():
+    prob = W.small_case(seed=35, M=3, nt=128, n_steps=23)
+    snaps, _ = mo.snapshots(prob, 4, z_mode=0)
+    assert mo.rel_l2_per_mode(snaps[-1], mo.solve(prob)).max() < 1e-13
+
+
 def test_pair_quirk_is_active_for_lexicographic_grin2():
     s = mo.OracleSolver(W.grin2(nt=64, n_steps=10))
     assert s.unique_pairs == [0, 2, 1, 3]
