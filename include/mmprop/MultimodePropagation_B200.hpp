@@ -105,6 +105,32 @@ class MultimodePropagationB200 : public MultimodePropagation {
     return e;
   }
 
+  // The MEX front end's n_save loop (matlab/mm_propagation.cpp:61-91): the result
+  // after each of n_save chunks of n_steps / n_save steps (the last one takes the
+  // remainder) with its position Z (m) and the seconds since the call began.
+  // referenceZ = true restarts z at each chunk as the reference's computeLawsonRK does;
+  // the default carries z on, so every snapshot is the field at its Z.
+  struct Snapshot {
+    double Z;
+    ComplexArraysContainer fields;
+    double cpu_time;
+  };
+  std::vector<Snapshot> computeSnapshots(unsigned int n_save, bool referenceZ = false) {
+    std::vector<double> f((size_t)2 * M_ * nt_ * (n_save ? n_save : 1)), z(n_save ? n_save : 1),
+        t(n_save ? n_save : 1);
+    check(mmp_propagate_snapshots(s_, n_save, referenceZ ? 1 : 0, f.data(), z.data(), t.data()),
+          "computeSnapshots");
+    std::vector<Snapshot> out;
+    for (unsigned i = 0; i < n_save; ++i) {
+      ComplexArraysContainer phi(nt_, M_);
+      const double* a = f.data() + (size_t)i * 2 * M_ * nt_;
+      for (unsigned p = 0; p < M_; ++p)
+        for (unsigned s = 0; s < nt_; ++s) phi[p][s] = Complex(a[2 * ((size_t)p * nt_ + s)], a[2 * ((size_t)p * nt_ + s) + 1]);
+      out.push_back(Snapshot{z[i], phi, t[i]});
+    }
+    return out;
+  }
+
   mmp_solver* handle() { return s_; }
 
  private:
