@@ -74,6 +74,8 @@ class mmp_info(C.Structure):
         ("steps_done", C.c_uint64),
         ("fp64", C.c_uint32),
         ("cluster_ctas", C.c_uint32),
+        ("raman_recurrence", C.c_uint32),
+        ("graph_branches", C.c_uint32),
     ]
 
 

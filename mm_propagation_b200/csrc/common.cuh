@@ -113,6 +113,14 @@ struct SolveDesc {
   // Stage kernels do nothing for this solve once *step >= step_limit (a solve in a
   // served pool stops at its own step count while the pool's graph keeps running).
   unsigned long long step_limit;
+  // Raman response as a damped sinusoid h_i = Im(c lambda^i) (k_raman_scan): iir = 1
+  // when the sampled h_R fits it; kappa = Delta_t T0 f_R c (1 - lambda^NT),
+  // inv_one_minus = 1 / (1 - lambda^NT).
+  int iir;
+  int pad2_;
+  double2 iir_lambda;
+  double2 iir_kappa;
+  double2 iir_inv_one_minus;
 };
 
 // RK tableau passed by value to the stage kernels (identical for a batch).

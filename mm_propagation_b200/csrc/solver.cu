@@ -8,6 +8,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -96,6 +97,9 @@ namespace {
     }                                                                                    \
   } while (0)
 
+// shared memory of k_raman_scan: a 128 KB segment of V, padded
+constexpr int kScanSmem = padded_len(128 * 1024 / 8) * 8;
+
 // ---- per-device resources: twiddle tables, kernel attributes ------------------------------
 struct DeviceRes {
   bool ready = false;
@@ -155,6 +159,10 @@ int ensure_device(int dev, DeviceRes** out) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<double>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   r.ready = true;
   *out = &r;
   return MMP_OK;
@@ -461,6 +469,7 @@ struct mmp_batch {
   cudaMemPool_t mempool = nullptr;
   // graph branches: solves split into `groups` independent kernel chains (capture_steps)
   uint32_t groups = 1;
+  bool raman_iir = false;  // every solve's h_R is a damped sinusoid: pair fields by k_raman_scan
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -555,6 +564,25 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   return MMP_OK;
 }
 
+// Raman pair fields for `nsolves` solves from descs: the recurrence scan when every
+// solve's h_R is a damped sinusoid, else the FFT convolution of kernel set ks.
+int launch_pairs(mmp_batch* b, const KernelSet& ks, int nsolves, int stage, const SolveDesc* descs,
+                 cudaStream_t st = nullptr) {
+  if (!(b->raman && b->Pmax > 0) || nsolves <= 0) return MMP_OK;
+  if (!b->raman_iir) return launch_row_kernel(b, ks, ks.pair, b->Pmax, nsolves, stage, descs, st);
+  int nt = (int)b->nt;
+  // segments of at most 128 KB of V staged in shared memory
+  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+  int seg = std::min(nt, (int)((128 * 1024) / t2));
+  const int thr = std::max(32, std::min(512, seg / 8));
+  const int smem = padded_len(seg) * (int)t2;
+  const SolveDesc* dd = descs;
+  void* args[] = {(void*)&dd, &nt, &seg};
+  const void* fn = b->fp64 ? (const void*)&k_raman_scan<double> : (const void*)&k_raman_scan<float>;
+  CUDA_TRY(launch(fn, dim3((unsigned)b->Pmax, (unsigned)nsolves, 1), thr, smem, 1, st ? st : b->stream, args));
+  return MMP_OK;
+}
+
 // ---- autotuner: rows on one CTA (or the minimal cluster) vs split over twice as many
 // CTAs. Both variants' pair and per-mode kernels are timed on this batch's own buffers
 // at stage 0 (which rewrites only W, U and N_hat_0: all of them are recomputed before
@@ -570,7 +598,7 @@ int time_variant(mmp_batch* b, const KernelSet& ks, float* ms) {
   int rc = MMP_OK;
   for (int rep = 0; rep < 4 && rc == MMP_OK; ++rep) {  // rep 0 warms up
     if (rep == 1) cudaEventRecord(e0, b->stream);
-    if (b->raman && b->Pmax > 0) rc = launch_row_kernel(b, ks, ks.pair, b->Pmax, nsol, 0, b->d_descs);
+    rc = launch_pairs(b, ks, nsol, 0, b->d_descs);
     if (rc == MMP_OK) rc = launch_row_kernel(b, ks, ks.nu, b->Mmax, nsol, 0, b->d_descs);
   }
   cudaEventRecord(e1, b->stream);
@@ -620,11 +648,8 @@ int enqueue_step(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cudaStr
   if (count == ~0u) count = b->span;
   const SolveDesc* descs = b->d_descs + first;
   for (int i = 0; i < b->tab.s; ++i) {
-    int rc;
-    if (b->raman && b->Pmax > 0) {
-      rc = launch_row_kernel(b, b->ks, b->ks.pair, b->Pmax, (int)count, i, descs, st);
-      if (rc) return rc;
-    }
+    int rc = launch_pairs(b, b->ks, (int)count, i, descs, st);
+    if (rc) return rc;
     rc = launch_contract(b, first, count, st);
     if (rc) return rc;
     rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, (int)count, i, descs, st);
@@ -840,6 +865,39 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   return off;
 }
 
+// Does the sampled Raman response satisfy h_i = Im(c lambda^i) for every i < n (a damped
+// sinusoid, |lambda| < 1)? Then its circular convolution is a periodic first-order
+// recurrence (k_raman_scan). lambda is the complex root of z^2 = alpha z + beta, the
+// recurrence h_i = alpha h_{i-1} + beta h_{i-2} read off h_0..h_3; c follows from h_0, h_1.
+// Accepted when every sample matches the model to 1e-10 of max|h| (the sampled model
+// itself, evaluated in FP64, matches to ~1e-12 at NT = 2^16).
+bool fit_damped_sinusoid(const double* h, uint32_t n, std::complex<double>& lam, std::complex<double>& c) {
+  if (n < 16) return false;
+  double hmax = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!std::isfinite(h[i])) return false;
+    hmax = std::max(hmax, std::fabs(h[i]));
+  }
+  if (hmax == 0) return false;
+  const double det = h[1] * h[1] - h[0] * h[2];
+  if (std::fabs(det) < 1e-300) return false;
+  const double alpha = (h[2] * h[1] - h[3] * h[0]) / det;
+  const double beta = (h[1] * h[3] - h[2] * h[2]) / det;
+  const double disc = alpha * alpha + 4 * beta;
+  if (!(disc < 0)) return false;  // real roots: not an oscillating response
+  lam = std::complex<double>(alpha / 2, std::sqrt(-disc) / 2);
+  if (!(std::abs(lam) < 1)) return false;
+  // Im(c) = h_0, Im(c lambda) = c.re lambda.im + c.im lambda.re = h_1
+  c = std::complex<double>((h[1] - h[0] * lam.real()) / lam.imag(), h[0]);
+  std::complex<double> m = c;
+  const double tol = 1e-10 * hmax;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (std::fabs(h[i] - m.imag()) > tol) return false;
+    m *= lam;
+  }
+  return true;
+}
+
 // Host setup, device state and uploads for slot idx from params p; leaves the solve
 // at z = 0 with its initial fields transformed. One cudaMalloc for all of it.
 int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
@@ -903,6 +961,19 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.status = (int*)(s.counters + 3);
   d.monitors = (s.flags & MMP_F_NO_MONITORS) ? 0 : 1;
   d.step_limit = ~0ull;
+  if (b->raman) {
+    std::complex<double> lam, c;
+    if (fit_damped_sinusoid(p->raman_response, (uint32_t)nt, lam, c)) {
+      // R = w sum_i h_i V[n - i], w = Delta_t T0 f_R (the scale the spectrum H carries)
+      const std::complex<double> lamN = std::pow(lam, (double)nt);
+      const std::complex<double> kap = (s.delta_t * s.T0 * s.fR) * c * (1.0 - lamN);
+      const std::complex<double> inv = 1.0 / (1.0 - lamN);
+      d.iir = 1;
+      d.iir_lambda = make_double2(lam.real(), lam.imag());
+      d.iir_kappa = make_double2(kap.real(), kap.imag());
+      d.iir_inv_one_minus = make_double2(inv.real(), inv.imag());
+    }
+  }
   CUDA_TRY(cudaMemcpyAsync((void*)d.poly, s.poly.data(), s.poly.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
   if (P) CUDA_TRY(cudaMemcpyAsync((void*)d.pairs, s.pairs.data(), P * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
   if (!s.terms.empty())
@@ -943,29 +1014,38 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
 // its shared memory. Returns true when it changed (captured graphs are then stale).
 bool batch_shape(mmp_batch* b) {
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
-  int Mmax = 0, Pmax = 0;
+  int Mmax = 0, Pmax = 0, Pall = 0;
   uint32_t span = 0;
   size_t max_terms = 0;
+  bool iir = b->raman;
   for (size_t i = 0; i < b->members.size(); ++i) {
     if (!b->active[i]) continue;
     const Member& s = b->members[i];
+    iir = iir && s.desc.iir;
     span = (uint32_t)i + 1;
     Mmax = std::max(Mmax, (int)s.M);
     Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
+    Pall = std::max(Pall, (int)s.pairs.size());
     max_terms = std::max(max_terms, s.terms.size());
   }
-  // contraction tile: the largest power of two <= 256 whose U + R tile fits in 100 KB
-  const int rows = std::max(Mmax + Pmax, 1);
+  // contraction tile: the largest power of two <= 256 whose U + pair-field tile fits in
+  // 100 KB (the pair fields are formed in the tile with Raman on and off)
+  const int rows = std::max(Mmax + Pall, 1);
   int TT = 256;
   while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
   while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
   while (TT > (int)b->nt) TT >>= 1;
   size_t smem = (size_t)rows * TT * t2;
-  // terms follow the tiles in shared memory when they fit (else they are read through L1)
-  const int stage_terms = smem + max_terms * sizeof(Term) <= 200 * 1024 ? 1 : 0;
-  if (stage_terms) smem += max_terms * sizeof(Term);
+  // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
+  // are read through L1 from the FP64 table)
+  const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);
+  const int stage_terms = smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
+  if (stage_terms) smem += max_terms * staged;
+  if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
+    if (std::atoi(env) == 1) iir = false;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
-                       stage_terms != b->stage_terms || span != b->span;
+                       stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir;
+  b->raman_iir = iir;
   b->span = span;
   b->Mmax = Mmax;
   b->Pmax = Pmax;
@@ -1039,6 +1119,8 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->steps_done = s.total_host;
   info->fp64 = b->fp64 ? 1u : 0u;
   info->cluster_ctas = (uint32_t)b->ks.C;
+  info->raman_recurrence = b->raman_iir ? 1u : 0u;
+  info->graph_branches = b->groups;
 }
 
 }  // namespace
@@ -1138,7 +1220,7 @@ int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t
         if (kind == 0 && !(b->raman && b->Pmax > 0)) continue;
         cudaError_t e = cudaEventRecord(ev[0], b->stream);
         if (e != cudaSuccess) { rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
-        if (kind == 0) rc = launch_row_kernel(b, b->ks, b->ks.pair, b->Pmax, nsol, i, b->d_descs);
+        if (kind == 0) rc = launch_pairs(b, b->ks, nsol, i, b->d_descs);
         else if (kind == 1) rc = launch_contract(b);
         else rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, nsol, i, b->d_descs);
         if (rc) break;

@@ -72,6 +72,28 @@ template <typename T> __device__ __forceinline__ c2<T> expi(double theta) {
 template <typename T> __device__ __forceinline__ c2<T>* as_t2(void* p) { return reinterpret_cast<c2<T>*>(p); }
 template <typename T> __device__ __forceinline__ const c2<T>* as_t2(const void* p) { return reinterpret_cast<const c2<T>*>(p); }
 
+// two adjacent complex samples (one 16-byte access in FP32; p 16-byte aligned)
+template <typename T>
+__device__ __forceinline__ void ld2(const c2<T>* p, c2<T>& a, c2<T>& b) {
+  a = p[0];
+  b = p[1];
+}
+template <>
+__device__ __forceinline__ void ld2<float>(const float2* p, float2& a, float2& b) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  a = make_float2(v.x, v.y);
+  b = make_float2(v.z, v.w);
+}
+template <typename T>
+__device__ __forceinline__ void st2(c2<T>* p, c2<T> a, c2<T> b) {
+  p[0] = a;
+  p[1] = b;
+}
+template <>
+__device__ __forceinline__ void st2<float>(float2* p, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+
 __device__ __forceinline__ void load_poly(double* poly, const SolveDesc& d, int p) {
   if (threadIdx.x < d.n_beta) poly[threadIdx.x] = d.poly[p * d.n_beta + threadIdx.x];
   __syncthreads();
@@ -83,9 +105,8 @@ __device__ __forceinline__ void load_poly(double* poly, const SolveDesc& d, int 
 static_assert(sizeof(SolveDesc) % 8 == 0, "descriptor copied in 8-byte words");
 __device__ __forceinline__ void stage_desc(SolveDesc* dst, const SolveDesc* src) {
   constexpr int W = (int)(sizeof(SolveDesc) / 8);
-  if (threadIdx.x < W)
-    reinterpret_cast<unsigned long long*>(dst)[threadIdx.x] =
-        __ldg(reinterpret_cast<const unsigned long long*>(src) + threadIdx.x);
+  for (int i = threadIdx.x; i < W; i += blockDim.x)
+    reinterpret_cast<unsigned long long*>(dst)[i] = __ldg(reinterpret_cast<const unsigned long long*>(src) + i);
 }
 
 // Ask the TMA engine to pull [p, p + bytes) into L2 without waiting for it
@@ -210,6 +231,199 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   V* R = as_t2<T>(d.W) + (size_t)q * Gm::N;
 #pragma unroll 8
   for (int u = tid; u < Gm::NL; u += Gm::NTHR) R[Gm::time_of(rank, u)] = s[pad(u)];
+}
+
+// ---- k_raman_scan: R_q = h_R (*) V_q as a periodic linear recurrence ----------------------
+// Used instead of k_pair when the sampled Raman response is a damped sinusoid,
+// h_i = Im(c lambda^i) for every i < NT (the model simulations/main.cpp:67-75 samples;
+// the host checks the fit to 1e-10 of max|h|). With V = a + i b (a, b real) and
+// w = Delta_t T0 f_R,
+//   R[n] = w sum_i h_i V[(n - i) mod NT] = Im(kappa S_a[n]) + i Im(kappa S_b[n]),
+//   S[n] = lambda S[n-1] + x[n]  (x = a or b, periodic in n), kappa = w c (1 - lambda^NT):
+// the same circular convolution k_pair evaluates by FFT, in O(NT) per row.
+// Each thread owns E consecutive samples in sub-chunks of 8. Sub-chunk scans run in T
+// from zero; carries between sub-chunks and threads are FP64: a block-wide scan of
+// the affine maps s -> A s + B (A = lambda^E) gives every thread the state entering its
+// samples, and the periodic start S[-1] = S_lin[NT-1] / (1 - lambda^NT) closes the circle.
+struct Affine {  // s -> a s + (ba, bb) for the two scans
+  double2 a, ba, bb;
+};
+__device__ __forceinline__ Affine affine_then(const Affine& first, const Affine& second) {
+  Affine r;
+  r.a = cmul(first.a, second.a);
+  r.ba = cadd(cmul(second.a, first.ba), second.ba);
+  r.bb = cadd(cmul(second.a, first.bb), second.bb);
+  return r;
+}
+__device__ __forceinline__ double2 shfl_up_d2(double2 v, int off, unsigned mask) {
+  v.x = __shfl_up_sync(mask, v.x, off);
+  v.y = __shfl_up_sync(mask, v.y, off);
+  return v;
+}
+__device__ __forceinline__ Affine shfl_up_affine(const Affine& v, int off, unsigned mask) {
+  Affine r;
+  r.a = shfl_up_d2(v.a, off, mask);
+  r.ba = shfl_up_d2(v.ba, off, mask);
+  r.bb = shfl_up_d2(v.bb, off, mask);
+  return r;
+}
+// inclusive scan over the lanes of a warp (lanes >= n hold identities)
+__device__ __forceinline__ Affine warp_scan_affine(Affine v, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const Affine o = shfl_up_affine(v, off, 0xffffffffu);
+    if (lane >= off) v = affine_then(o, v);
+  }
+  return v;
+}
+
+// Block-wide exclusive scan of the threads' maps (in thread order): returns the map of
+// all earlier threads; *total receives the composition over the whole block.
+__device__ __forceinline__ Affine block_scan_affine(const Affine& mine, Affine* warp_tot, Affine* total) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const Affine incl = warp_scan_affine(mine, lane);
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  Affine wpre;  // maps of all earlier warps
+  wpre.a = make_double2(1.0, 0.0);
+  wpre.ba = wpre.bb = make_double2(0.0, 0.0);
+  for (int w = 0; w < warp; ++w) wpre = affine_then(wpre, warp_tot[w]);
+  Affine t = wpre;
+  for (int w = warp; w < nwarps; ++w) t = affine_then(t, warp_tot[w]);
+  *total = t;
+  Affine lpre = shfl_up_affine(incl, 1, 0xffffffffu);  // earlier lanes of this warp
+  if (lane == 0) {
+    lpre.a = make_double2(1.0, 0.0);
+    lpre.ba = lpre.bb = make_double2(0.0, 0.0);
+  }
+  __syncthreads();  // warp_tot is reused by the next scan
+  return affine_then(wpre, lpre);
+}
+
+// Rows are processed in segments of `seg` samples (the whole row when it fits the
+// 128 KB staging buffer): V = U_l conj(U_m) of a segment is formed in shared memory from
+// coalesced loads, every thread scans its E consecutive samples from there, and the
+// outputs are written back in place and stored coalesced. With one segment the staged
+// V serves both passes; with several, pass 1 records each segment's map and pass 2
+// stages every segment again.
+template <typename T>
+__global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict__ descs, int nt, int seg) {
+  using V = c2<T>;
+  constexpr int kMaxSeg = 16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* sv = reinterpret_cast<V*>(smem_raw);  // padded: element i at pad(i)
+  __shared__ Affine warp_tot[16];
+  __shared__ Affine seg_map[kMaxSeg];
+  const SolveDesc& d = descs[blockIdx.y];
+  const int q = blockIdx.x;
+  if (q >= d.P || __ldcg(d.step) >= d.step_limit) return;  // uniform over the CTA
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;                   // 32..512, a power of two
+  const int nseg = nt / seg;                     // <= kMaxSeg
+  const int act = min(nthr, seg >> 3);           // threads that own samples
+  const int E = seg / act;                       // a multiple of 8
+  const int myE = tid < act ? E : 0;
+  const int off = min(tid, act - 1) * E;
+  const int2 lm = d.pairs[q];
+  const V* Ul = as_t2<T>(d.U) + (size_t)lm.x * nt;
+  const V* Um = as_t2<T>(d.U) + (size_t)lm.y * nt;
+  V* R = as_t2<T>(d.W) + (size_t)q * nt;
+  const double2 lam = d.iir_lambda;
+  V pw[8];  // lambda^(k+1)
+  double2 lam8;
+  {
+    double2 p = lam;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      pw[k] = from_d2<T>(p);
+      lam8 = p;
+      p = cmul(p, lam);
+    }
+  }
+  const V lt = from_d2<T>(lam);
+  // stage V of segment g into shared memory (coalesced: two samples per thread per load)
+  auto stage = [&](int g) {
+    const size_t base = (size_t)g * seg;
+    for (int i2 = tid; i2 < (seg >> 1); i2 += nthr) {
+      V ul0, ul1, um0, um1;
+      ld2<T>(Ul + base + 2 * i2, ul0, ul1);
+      ld2<T>(Um + base + 2 * i2, um0, um1);
+      sv[pad(2 * i2)] = cmulc(ul0, um0);
+      sv[pad(2 * i2 + 1)] = cmulc(ul1, um1);
+    }
+    __syncthreads();
+  };
+  // this thread's map s -> lambda^E s + (S_a, S_b) over its samples of the staged segment
+  auto thread_map = [&]() {
+    Affine mine;
+    mine.a = make_double2(1.0, 0.0);
+    mine.ba = make_double2(0.0, 0.0);
+    mine.bb = make_double2(0.0, 0.0);
+    for (int j = 0; j < myE; j += 8) {
+      V la = mk<T>(0, 0), lb = mk<T>(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const V x = sv[pad(off + j + k)];
+        la = cmul(lt, la); la.x += x.x;
+        lb = cmul(lt, lb); lb.x += x.y;
+      }
+      mine.a = cmul(mine.a, lam8);
+      mine.ba = cadd(cmul(lam8, mine.ba), to_d2(la));
+      mine.bb = cadd(cmul(lam8, mine.bb), to_d2(lb));
+    }
+    return mine;
+  };
+  // pass 1: every segment's map (a single segment stays staged for pass 2)
+  Affine pre, tot;
+  for (int g = 0; g < nseg; ++g) {
+    stage(g);
+    pre = block_scan_affine(thread_map(), warp_tot, &tot);
+    if (tid == 0) seg_map[g] = tot;
+    if (nseg > 1) __syncthreads();  // the next segment overwrites sv
+  }
+  __syncthreads();
+  // periodic start: S[-1] = S_lin[NT-1] / (1 - lambda^NT)
+  Affine row;
+  row.a = make_double2(1.0, 0.0);
+  row.ba = row.bb = make_double2(0.0, 0.0);
+  for (int g = 0; g < nseg; ++g) row = affine_then(row, seg_map[g]);
+  const double2 inv = d.iir_inv_one_minus;
+  double2 sa = cmul(row.ba, inv), sb = cmul(row.bb, inv);  // state entering segment 0
+  const double2 kap = d.iir_kappa;
+  const V kt = from_d2<T>(kap);
+  // pass 2: outputs R = Im(kappa s), s = local + lambda^(k+1) C within each sub-chunk
+  for (int g = 0; g < nseg; ++g) {
+    if (nseg > 1) {
+      stage(g);
+      pre = block_scan_affine(thread_map(), warp_tot, &tot);
+    }
+    double2 Ca = cadd(cmul(pre.a, sa), pre.ba);
+    double2 Cb = cadd(cmul(pre.a, sb), pre.bb);
+    for (int j = 0; j < myE; j += 8) {
+      const V kca = from_d2<T>(cmul(kap, Ca)), kcb = from_d2<T>(cmul(kap, Cb));
+      V la = mk<T>(0, 0), lb = mk<T>(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        V& cell = sv[pad(off + j + k)];
+        const V x = cell;
+        la = cmul(lt, la); la.x += x.x;
+        lb = cmul(lt, lb); lb.x += x.y;
+        const V ca = cmul(pw[k], kca), cb = cmul(pw[k], kcb);
+        cell = mk<T>(kt.x * la.y + kt.y * la.x + ca.y, kt.x * lb.y + kt.y * lb.x + cb.y);
+      }
+      Ca = cadd(cmul(lam8, Ca), to_d2(la));
+      Cb = cadd(cmul(lam8, Cb), to_d2(lb));
+    }
+    __syncthreads();
+    const size_t base = (size_t)g * seg;
+    for (int i2 = tid; i2 < (seg >> 1); i2 += nthr) st2<T>(R + base + 2 * i2, sv[pad(2 * i2)], sv[pad(2 * i2 + 1)]);
+    // state entering the next segment
+    const double2 na = cadd(cmul(seg_map[g].a, sa), seg_map[g].ba);
+    const double2 nb = cadd(cmul(seg_map[g].a, sb), seg_map[g].bb);
+    sa = na;
+    sb = nb;
+    if (nseg > 1) __syncthreads();
+  }
 }
 
 // ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
@@ -569,15 +783,27 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 constexpr unsigned kMaxWaitPolls = 1u << 24;  // far above any copy time; then report, not hang
 
 // ---- k_contract: sigma_p(t) = sum_terms Q U_k(t) W(t) over a tile of t, all p ----------
-// The U tile [M][TT] and the W tile [P][TT] (Raman on) arrive in shared memory as
+// The U tile [M][TT] and the R tile [P][TT] (Raman on) arrive in shared memory as
 // one bulk-async copy per row segment (TT contiguous samples), issued by the
-// threads of the CTA and counted on one mbarrier. A warp then covers 32
-// consecutive t of one p, so term reads are warp-uniform and tile reads are
-// conflict-free.
+// threads of the CTA and counted on one mbarrier. Then
+//   1. every pair field of the tile is formed once, in place:
+//        W_lm = (1 - f_R) U_l conj(U_m) + R_lm      (Raman off: U_l conj(U_m)),
+//   2. each thread accumulates sigma_p for two adjacent samples over p's terms,
+//        sigma_p += q U_k W_pair   (conj(W_pair) for terms whose (l, m) is (m, l) of the
+//        stored pair: R_ml = conj(R_lm) as h_R is real, and the Kerr part likewise).
+// A warp covers 64 consecutive t of one p (TT >= 64), so term reads are warp-uniform
+// and tile reads are conflict-free; terms are staged in shared memory with the
+// coefficient already in T.
+template <typename T> struct StagedTerm {
+  unsigned short k, pc;
+  T q;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
                                                   int stage_terms) {
   using V = c2<T>;
+  using ST = StagedTerm<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bar;
   V* sU = reinterpret_cast<V*>(smem_raw);
@@ -586,26 +812,32 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;  // empty slot / finished
   const int M = d.M;
   const int raman = d.raman;
-  const int P = raman ? d.P : 0;
+  const int P = d.P;                  // pair fields formed in this tile
+  const int Pl = raman ? P : 0;       // pair rows loaded (Raman convolutions)
   const T kerr = (T)d.one_minus_fR;
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
-  const Term* terms = d.terms;
+  ST* st = reinterpret_cast<ST*>(sU + (size_t)(M + P) * TT);
   if (stage_terms) {
-    Term* st = reinterpret_cast<Term*>(sU + (size_t)(M + P) * TT);
-    for (int j = threadIdx.x; j < n_terms; j += blockDim.x) st[j] = d.terms[j];
-    terms = st;
+    for (int j = threadIdx.x; j < n_terms; j += blockDim.x) {
+      const Term tm = d.terms[j];
+      ST s;
+      s.k = tm.k;
+      s.pc = tm.pc;
+      s.q = (T)tm.q;
+      st[j] = s;
+    }
   }
   const V* U = as_t2<T>(d.U);
-  const V* W = as_t2<T>(d.W);
+  const V* R = as_t2<T>(d.W);
   const unsigned row_bytes = (unsigned)(TT * sizeof(V));
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, (unsigned)(M + P) * row_bytes);
+    mbar_arrive_expect_tx(&bar, (unsigned)(M + Pl) * row_bytes);
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < M + P; r += blockDim.x) {
-    const V* src = (r < M) ? U + (size_t)r * nt + t0 : W + (size_t)(r - M) * nt + t0;
+  for (int r = threadIdx.x; r < M + Pl; r += blockDim.x) {
+    const V* src = (r < M) ? U + (size_t)r * nt + t0 : R + (size_t)(r - M) * nt + t0;
     bulk_g2s(sU + (size_t)r * TT, src, row_bytes, &bar);
   }
   // every thread polls with a bound; the barrier makes the outcome CTA-uniform and
@@ -617,25 +849,54 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
     mbar_wait(&bar, 0, kMaxWaitPolls);
     return;
   }
+  const int H = TT >> 1;  // sample pairs per row
+  // 1. pair fields, two samples per thread
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int q = idx / H, tt = 2 * (idx - q * H);
+    const int2 lm = d.pairs[q];
+    V ul0, ul1, um0, um1;
+    ld2<T>(sU + lm.x * TT + tt, ul0, ul1);
+    ld2<T>(sU + lm.y * TT + tt, um0, um1);
+    V w0 = cmulc(ul0, um0), w1 = cmulc(ul1, um1);
+    if (raman) {
+      V r0, r1;
+      ld2<T>(sW + q * TT + tt, r0, r1);
+      w0 = mk<T>(fma(kerr, w0.x, r0.x), fma(kerr, w0.y, r0.y));
+      w1 = mk<T>(fma(kerr, w1.x, r1.x), fma(kerr, w1.y, r1.y));
+    }
+    st2<T>(sW + q * TT + tt, w0, w1);
+  }
+  __syncthreads();
+  // 2. contraction
   V* sigma = as_t2<T>(d.sigma);
-  for (int idx = threadIdx.x; idx < M * TT; idx += blockDim.x) {
-    const int p = idx / TT, tt = idx - p * TT;
-    T ax = 0, ay = 0;
+  for (int idx = threadIdx.x; idx < M * H; idx += blockDim.x) {
+    const int p = idx / H, tt = 2 * (idx - p * H);
+    T ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
     const int j1 = d.term_off[p + 1];
     for (int j = d.term_off[p]; j < j1; ++j) {
-      const Term tm = terms[j];
-      V w = cmulc(sU[tm.l * TT + tt], sU[tm.m * TT + tt]);
-      if (raman) {
-        V r = sW[(tm.pc & 0x7fff) * TT + tt];
-        if (tm.pc & 0x8000) r.y = -r.y;
-        w = cadd(cscale(w, kerr), r);
+      unsigned short k, pc;
+      T qv;
+      if (stage_terms) {
+        const ST s = st[j];
+        k = s.k; pc = s.pc; qv = s.q;
+      } else {
+        const Term tm = d.terms[j];
+        k = tm.k; pc = tm.pc; qv = (T)tm.q;
       }
-      const V uw = cmul(sU[tm.k * TT + tt], w);
-      const T qv = (T)tm.q;
-      ax = fma(qv, uw.x, ax);
-      ay = fma(qv, uw.y, ay);
+      V u0, u1, w0, w1;
+      ld2<T>(sU + k * TT + tt, u0, u1);
+      ld2<T>(sW + (pc & 0x7fff) * TT + tt, w0, w1);
+      if (pc & 0x8000) {
+        w0.y = -w0.y;
+        w1.y = -w1.y;
+      }
+      const V a0 = cmul(u0, w0), a1 = cmul(u1, w1);
+      ax0 = fma(qv, a0.x, ax0);
+      ay0 = fma(qv, a0.y, ay0);
+      ax1 = fma(qv, a1.x, ax1);
+      ay1 = fma(qv, a1.y, ay1);
     }
-    sigma[(size_t)p * nt + t0 + tt] = mk<T>(ax, ay);
+    st2<T>(sigma + (size_t)p * nt + t0 + tt, mk<T>(ax0, ay0), mk<T>(ax1, ay1));
   }
 }
 

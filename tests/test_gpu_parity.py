@@ -159,3 +159,38 @@ def test_grin6_full_rows_live(mmp):
     b, _ = run(mmp, prob, [8], capi.MMP_F_FP64)
     assert mo.rel_l2_per_mode(b, ref).max() < TOL64
     assert mo.rel_l2_per_mode(a, ref).max() < TOL32
+
+
+def two_term_response(nt, window):
+    """A Raman response that is not one damped sinusoid (two of them): the solver must
+    take the FFT convolution for it."""
+    dt = window / nt
+    t = np.arange(nt) * dt
+    h = np.exp(-t / 0.032) * np.sin(t / 0.0122) + 0.3 * np.exp(-t / 0.1) * np.sin(t / 0.05)
+    return h / (h.sum() * dt)
+
+
+@pytest.mark.parametrize("fp64", [True, False])
+def test_raman_fft_path_for_a_general_response(mmp, fp64):
+    prob = W.small_case(seed=90, M=3, nt=1024, n_steps=8)
+    prob = prob.replace(raman_response=two_term_response(1024, prob.time_window))
+    ref = mo.solve(prob)
+    out, info = run(mmp, prob, [8], capi.MMP_F_FP64 if fp64 else 0)
+    assert info["raman_recurrence"] == 0
+    assert mo.rel_l2_per_mode(out, ref).max() < (TOL64 if fp64 else TOL32)
+
+
+@pytest.mark.parametrize("fp64", [True, False])
+@pytest.mark.parametrize("nt,window", [(256, 10.0), (4096, 10.0), (65536, 40.0)])
+def test_raman_recurrence_matches_fft_convolution(mmp, monkeypatch, fp64, nt, window):
+    # h_R of the reference driver's form: the recurrence path, checked against the FFT
+    # path on the same solve and against the oracle
+    prob = W.small_case(seed=91, M=3, nt=nt, n_steps=6, window=window, nnz_target=10)
+    fl = capi.MMP_F_FP64 if fp64 else 0
+    out_r, info_r = run(mmp, prob, [6], fl)
+    monkeypatch.setenv("MMP_RAMAN_FFT", "1")
+    out_f, info_f = run(mmp, prob, [6], fl)
+    assert (info_r["raman_recurrence"], info_f["raman_recurrence"]) == (1, 0)
+    assert mo.rel_l2_per_mode(out_r, out_f).max() < (1e-12 if fp64 else 2e-6)
+    ref = mo.solve(prob)
+    assert mo.rel_l2_per_mode(out_r, ref).max() < (TOL64 if fp64 else TOL32)
