@@ -105,8 +105,9 @@ typedef struct mmp_info {
   uint64_t steps_done;                      /* steps since creation (monotone) */
   uint32_t fp64;                            /* 1 if MMP_F_FP64 */
   uint32_t cluster_ctas;                    /* CTAs that share one FFT row */
-  uint32_t raman_recurrence;                /* 1: Raman convolution as a recurrence (h_R is a
-                                               damped sinusoid h_i = Im(c lambda^i)); 0: by FFT */
+  uint32_t raman_recurrence;                /* Raman convolution: 0 by FFT; as a recurrence (h_R
+                                               a damped sinusoid h_i = Im(c lambda^i)) 1 in a row
+                                               pass, 2 inside the contraction tiles */
   uint32_t graph_branches;                  /* independent solve groups per captured graph */
 } mmp_info;
 

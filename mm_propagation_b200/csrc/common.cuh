@@ -121,6 +121,9 @@ struct SolveDesc {
   double2 iir_lambda;
   double2 iir_kappa;
   double2 iir_inv_one_minus;
+  // [P][NT/16][2] (T complex): per contraction tile and pair field, the recurrence's
+  // tile aggregate (k_raman_agg), then the state entering the tile (k_raman_carry)
+  void* raman_tiles;
 };
 
 // RK tableau passed by value to the stage kernels (identical for a batch).

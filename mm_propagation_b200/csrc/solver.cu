@@ -163,6 +163,10 @@ int ensure_device(int dev, DeviceRes** out) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_agg<float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_agg<double>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   r.ready = true;
   *out = &r;
   return MMP_OK;
@@ -470,6 +474,7 @@ struct mmp_batch {
   // graph branches: solves split into `groups` independent kernel chains (capture_steps)
   uint32_t groups = 1;
   bool raman_iir = false;  // every solve's h_R is a damped sinusoid: pair fields by k_raman_scan
+  bool raman_fused = false;  // ... and the recurrence runs inside the contraction tiles
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -557,20 +562,34 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   if (count == 0) return MMP_OK;
   const SolveDesc* descs = b->d_descs + first;
   int nt = (int)b->nt, TT = b->TT, sterms = b->stage_terms;
-  void* args[] = {(void*)&descs, &nt, &TT, &sterms};
+  int mode = !b->raman ? 0 : (b->raman_fused ? 2 : 1);
+  void* args[] = {(void*)&descs, &nt, &TT, &sterms, &mode};
   dim3 grid((unsigned)(b->nt / b->TT), count, 1);
   const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, args));
   return MMP_OK;
 }
 
-// Raman pair fields for `nsolves` solves from descs: the recurrence scan when every
-// solve's h_R is a damped sinusoid, else the FFT convolution of kernel set ks.
+// Raman pair fields for `nsolves` solves from descs: with the recurrence fused into the
+// contraction, its tile aggregates and carries; else the recurrence as a row scan when
+// every solve's h_R is a damped sinusoid; else the FFT convolution of kernel set ks.
 int launch_pairs(mmp_batch* b, const KernelSet& ks, int nsolves, int stage, const SolveDesc* descs,
                  cudaStream_t st = nullptr) {
   if (!(b->raman && b->Pmax > 0) || nsolves <= 0) return MMP_OK;
   if (!b->raman_iir) return launch_row_kernel(b, ks, ks.pair, b->Pmax, nsolves, stage, descs, st);
   int nt = (int)b->nt;
+  if (b->raman_fused) {
+    const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+    int TT = b->TT;
+    const SolveDesc* dd = descs;
+    void* args[] = {(void*)&dd, &nt, &TT};
+    const int smem = (int)(((size_t)b->Mmax * TT + 8 * (size_t)padded_len(TT)) * t2);
+    const void* fa = b->fp64 ? (const void*)&k_raman_agg<double> : (const void*)&k_raman_agg<float>;
+    CUDA_TRY(launch(fa, dim3((unsigned)(nt / TT), (unsigned)nsolves, 1), 256, smem, 1, st ? st : b->stream, args));
+    const void* fc = b->fp64 ? (const void*)&k_raman_carry<double> : (const void*)&k_raman_carry<float>;
+    CUDA_TRY(launch(fc, dim3((unsigned)b->Pmax, (unsigned)nsolves, 1), 32, 0, 1, st ? st : b->stream, args));
+    return MMP_OK;
+  }
   // segments of at most 128 KB of V staged in shared memory
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   int seg = std::min(nt, (int)((128 * 1024) / t2));
@@ -857,6 +876,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + M * nt * t2);                                            // sigma
   off = align_up(off + (b->raman ? P : 0) * nt * t2);                           // W (R)
   off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));    // H
+  off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);                // Raman tile carries
   off = align_up(off + s.poly.size() * sizeof(double));
   off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -906,7 +926,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   host_setup(p, s);
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
-  // one allocation: psi_hat | io | Nh | U | sigma | W | H | poly | pairs | terms | term_off | counters
+  // one allocation: psi_hat | io | Nh | U | sigma | W | H | tiles | poly | pairs | terms | term_off | counters
   size_t off = 0;
   const size_t o_psi = off; off = align_up(off + M * nt * sizeof(double2));
   const size_t o_io = off; off = align_up(off + M * nt * sizeof(double2));
@@ -915,6 +935,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_sig = off; off = align_up(off + M * nt * t2);
   const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
   const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
+  const size_t o_rt = off; off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);
   const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
   const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -951,6 +972,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.sigma = T2ptr(s.block, o_sig);
   d.W = T2ptr(s.block, o_w);
   d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
+  d.raman_tiles = b->raman ? T2ptr(s.block, o_rt) : nullptr;
   d.pairs = (const int2*)T2ptr(s.block, o_pairs);
   d.terms = (const Term*)T2ptr(s.block, o_terms);
   d.term_off = (const int*)T2ptr(s.block, o_toff);
@@ -1036,16 +1058,27 @@ bool batch_shape(mmp_batch* b) {
   while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
   while (TT > (int)b->nt) TT >>= 1;
   size_t smem = (size_t)rows * TT * t2;
+  if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
+    if (std::atoi(env) == 1) iir = false;
+  // the recurrence runs inside the contraction tiles when a lane gets 2..8 samples
+  // (64 <= TT <= 256) and the per-warp scratch rows fit; MMP_RAMAN_FUSED=0 keeps the row scan
+  bool fused = iir && TT >= 64 && (int)b->nt >= TT;
+  const size_t scratch = 8 * (size_t)padded_len(TT) * t2;
+  if (fused && smem + scratch > 200 * 1024) fused = false;
+  if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
+    if (std::atoi(env) == 0) fused = false;
+  if (fused) smem += scratch;
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
   // are read through L1 from the FP64 table)
   const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);
   const int stage_terms = smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
   if (stage_terms) smem += max_terms * staged;
-  if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
-    if (std::atoi(env) == 1) iir = false;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
-                       stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir;
+                       stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
+                       fused != b->raman_fused;
   b->raman_iir = iir;
+  b->raman_fused = fused;
+  b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
   b->span = span;
   b->Mmax = Mmax;
   b->Pmax = Pmax;
@@ -1119,7 +1152,7 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->steps_done = s.total_host;
   info->fp64 = b->fp64 ? 1u : 0u;
   info->cluster_ctas = (uint32_t)b->ks.C;
-  info->raman_recurrence = b->raman_iir ? 1u : 0u;
+  info->raman_recurrence = b->raman_fused ? 2u : (b->raman_iir ? 1u : 0u);
   info->graph_branches = b->groups;
 }
 

@@ -279,23 +279,33 @@ __device__ __forceinline__ Affine warp_scan_affine(Affine v, int lane) {
 
 // Block-wide exclusive scan of the threads' maps (in thread order): returns the map of
 // all earlier threads; *total receives the composition over the whole block.
+__device__ __forceinline__ Affine affine_identity() {
+  Affine r;
+  r.a = make_double2(1.0, 0.0);
+  r.ba = r.bb = make_double2(0.0, 0.0);
+  return r;
+}
+// warp_tot holds 17 entries: per-warp totals, then (after the scan) per-warp exclusive
+// prefixes in [0, 16) and the block total in [16].
 __device__ __forceinline__ Affine block_scan_affine(const Affine& mine, Affine* warp_tot, Affine* total) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const Affine incl = warp_scan_affine(mine, lane);
   if (lane == 31) warp_tot[warp] = incl;
   __syncthreads();
-  Affine wpre;  // maps of all earlier warps
-  wpre.a = make_double2(1.0, 0.0);
-  wpre.ba = wpre.bb = make_double2(0.0, 0.0);
-  for (int w = 0; w < warp; ++w) wpre = affine_then(wpre, warp_tot[w]);
-  Affine t = wpre;
-  for (int w = warp; w < nwarps; ++w) t = affine_then(t, warp_tot[w]);
-  *total = t;
-  Affine lpre = shfl_up_affine(incl, 1, 0xffffffffu);  // earlier lanes of this warp
-  if (lane == 0) {
-    lpre.a = make_double2(1.0, 0.0);
-    lpre.ba = lpre.bb = make_double2(0.0, 0.0);
+  if (warp == 0) {  // one warp scans the warp totals
+    const Affine wt = lane < nwarps ? warp_tot[lane] : affine_identity();
+    const Affine wi = warp_scan_affine(wt, lane);
+    Affine we = shfl_up_affine(wi, 1, 0xffffffffu);
+    if (lane == 0) we = affine_identity();
+    __syncwarp();
+    if (lane < nwarps) warp_tot[lane] = we;
+    if (lane == 31) warp_tot[16] = wi;
   }
+  __syncthreads();
+  const Affine wpre = warp_tot[warp];
+  *total = warp_tot[16];
+  Affine lpre = shfl_up_affine(incl, 1, 0xffffffffu);  // earlier lanes of this warp
+  if (lane == 0) lpre = affine_identity();
   __syncthreads();  // warp_tot is reused by the next scan
   return affine_then(wpre, lpre);
 }
@@ -312,7 +322,7 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
   constexpr int kMaxSeg = 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* sv = reinterpret_cast<V*>(smem_raw);  // padded: element i at pad(i)
-  __shared__ Affine warp_tot[16];
+  __shared__ Affine warp_tot[17];
   __shared__ Affine seg_map[kMaxSeg];
   const SolveDesc& d = descs[blockIdx.y];
   const int q = blockIdx.x;
@@ -341,9 +351,14 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
     }
   }
   const V lt = from_d2<T>(lam);
+  // s <- lambda s + x for a real input x (two dependent FMAs per component)
+  auto step = [&](V s, T x) {
+    return mk<T>(fma(lt.x, s.x, fma(-lt.y, s.y, x)), fma(lt.x, s.y, lt.y * s.x));
+  };
   // stage V of segment g into shared memory (coalesced: two samples per thread per load)
   auto stage = [&](int g) {
     const size_t base = (size_t)g * seg;
+#pragma unroll 8
     for (int i2 = tid; i2 < (seg >> 1); i2 += nthr) {
       V ul0, ul1, um0, um1;
       ld2<T>(Ul + base + 2 * i2, ul0, ul1);
@@ -364,8 +379,8 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const V x = sv[pad(off + j + k)];
-        la = cmul(lt, la); la.x += x.x;
-        lb = cmul(lt, lb); lb.x += x.y;
+        la = step(la, x.x);
+        lb = step(lb, x.y);
       }
       mine.a = cmul(mine.a, lam8);
       mine.ba = cadd(cmul(lam8, mine.ba), to_d2(la));
@@ -406,10 +421,11 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
       for (int k = 0; k < 8; ++k) {
         V& cell = sv[pad(off + j + k)];
         const V x = cell;
-        la = cmul(lt, la); la.x += x.x;
-        lb = cmul(lt, lb); lb.x += x.y;
-        const V ca = cmul(pw[k], kca), cb = cmul(pw[k], kcb);
-        cell = mk<T>(kt.x * la.y + kt.y * la.x + ca.y, kt.x * lb.y + kt.y * lb.x + cb.y);
+        la = step(la, x.x);
+        lb = step(lb, x.y);
+        // Im(kappa local) + Im(lambda^(k+1) kappa C)
+        cell = mk<T>(fma(kt.x, la.y, fma(kt.y, la.x, fma(pw[k].x, kca.y, pw[k].y * kca.x))),
+                     fma(kt.x, lb.y, fma(kt.y, lb.x, fma(pw[k].x, kcb.y, pw[k].y * kcb.x))));
       }
       Ca = cadd(cmul(lam8, Ca), to_d2(la));
       Cb = cadd(cmul(lam8, Cb), to_d2(lb));
@@ -782,6 +798,171 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 }
 constexpr unsigned kMaxWaitPolls = 1u << 24;  // far above any copy time; then report, not hang
 
+// ---- the Raman recurrence inside a contraction tile ---------------------------------------
+// With h_R a damped sinusoid (see k_raman_scan) the pair fields' convolutions need no
+// row pass at all: per tile of TT = 32 c samples (2 <= c <= 8)
+//   k_raman_agg    the recurrence's aggregate over the tile from a zero start,
+//   k_raman_carry  per pair row, a scan of the tile aggregates (periodic start): the
+//                  state entering every tile,
+//   k_contract     (mode 2) runs the recurrence through its own tile from that state
+//                  and forms W = (1 - f_R) V + R in shared memory; R never leaves the SM.
+// Within a tile one warp handles one pair field at a time, lane L owning samples
+// [c L, c L + c); V is staged in a per-warp padded scratch row so that both the
+// coalesced fill (sample 32 j + L) and the lane-contiguous scan read without conflicts
+// beyond 2-way.
+template <typename T> struct TileScan {
+  using V = c2<T>;
+  V lt, kt;
+  V pw[8];      // lambda^(k+1)
+  V lvl[5];     // lambda^(c 2^j): the multipliers of the lane scan's levels
+  V lane_pow;   // lambda^(c lane): carries the tile's entering state to this lane
+  int c;
+  __device__ __forceinline__ void init(const SolveDesc& d, int c_, int lane) {
+    c = c_;
+    const double2 lam = d.iir_lambda;
+    lt = from_d2<T>(lam);
+    kt = from_d2<T>(d.iir_kappa);
+    double2 p = lam, lamc = lam;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      pw[k] = from_d2<T>(p);
+      if (k + 1 == c) lamc = p;
+      p = cmul(p, lam);
+    }
+    double2 lp = make_double2(1.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      lvl[j] = from_d2<T>(lamc);
+      if ((lane >> j) & 1) lp = cmul(lp, lamc);
+      lamc = cmul(lamc, lamc);
+    }
+    lane_pow = from_d2<T>(lp);
+  }
+  // inclusive scan over the lanes of (la, lb): s_L = lambda^c s_{L-1} + local_L
+  __device__ __forceinline__ void lane_scan(V& a, V& b, int lane) const {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int o = 1 << j;
+      V pa, pb;
+      pa.x = __shfl_up_sync(0xffffffffu, a.x, o);
+      pa.y = __shfl_up_sync(0xffffffffu, a.y, o);
+      pb.x = __shfl_up_sync(0xffffffffu, b.x, o);
+      pb.y = __shfl_up_sync(0xffffffffu, b.y, o);
+      if (lane >= o) {
+        a = cadd(cmul(lvl[j], pa), a);
+        b = cadd(cmul(lvl[j], pb), b);
+      }
+    }
+  }
+  __device__ __forceinline__ V step(V s, T x) const {
+    return mk<T>(fma(lt.x, s.x, fma(-lt.y, s.y, x)), fma(lt.x, s.y, lt.y * s.x));
+  }
+  // V = U_l conj(U_m) of the tile into the scratch row
+  __device__ __forceinline__ void form(const V* sU, int TT, int2 lm, V* scr, int lane) const {
+    for (int j = 0; j < c; ++j) {
+      const int e = 32 * j + lane;
+      scr[pad(e)] = cmulc(sU[lm.x * TT + e], sU[lm.y * TT + e]);
+    }
+  }
+  // this lane's recurrence over its samples from a zero start
+  __device__ __forceinline__ void lane_local(const V* scr, int lane, V& la, V& lb) const {
+    la = mk<T>(0, 0);
+    lb = mk<T>(0, 0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k < c) {
+        const V x = scr[pad(c * lane + k)];
+        la = step(la, x.x);
+        lb = step(lb, x.y);
+      }
+    }
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_u_tile(c2<T>* sU, const SolveDesc& d, int nt, int t0, int TT) {
+  const c2<T>* U = as_t2<T>(d.U);
+  const int H = TT >> 1;
+  for (int idx = threadIdx.x; idx < d.M * H; idx += blockDim.x) {
+    const int r = idx / H, tt = 2 * (idx - r * H);
+    c2<T> a, b;
+    ld2<T>(U + (size_t)r * nt + t0 + tt, a, b);
+    st2<T>(sU + r * TT + tt, a, b);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__ descs, int nt, int TT) {
+  using V = c2<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SolveDesc& d = descs[blockIdx.y];
+  const int tile = blockIdx.x, t0 = tile * TT;
+  if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  V* sU = reinterpret_cast<V*>(smem_raw);
+  V* scr = sU + (size_t)d.M * TT + (size_t)warp * padded_len(TT);
+  stage_u_tile<T>(sU, d, nt, t0, TT);
+  __syncthreads();
+  TileScan<T> ts;
+  ts.init(d, TT >> 5, lane);
+  const int ntiles = nt / TT;
+  V* out = as_t2<T>(d.raman_tiles);
+  for (int q = warp; q < d.P; q += nwarps) {
+    ts.form(sU, TT, d.pairs[q], scr, lane);
+    __syncwarp();
+    V la, lb;
+    ts.lane_local(scr, lane, la, lb);
+    ts.lane_scan(la, lb, lane);
+    if (lane == 31) {  // the whole tile
+      out[((size_t)q * ntiles + tile) * 2] = la;
+      out[((size_t)q * ntiles + tile) * 2 + 1] = lb;
+    }
+    __syncwarp();
+  }
+}
+
+// one warp per (pair field, solve): tile aggregates -> states entering the tiles
+template <typename T>
+__global__ void __launch_bounds__(32) k_raman_carry(const SolveDesc* __restrict__ descs, int nt, int TT) {
+  using V = c2<T>;
+  const SolveDesc& d = descs[blockIdx.y];
+  const int q = blockIdx.x;
+  if (q >= d.P || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;
+  const int lane = threadIdx.x;
+  const int ntiles = nt / TT;
+  const int per = (ntiles + 31) / 32;  // tiles per lane
+  const int first = min(lane * per, ntiles), last = min(first + per, ntiles);
+  double2 lamT = d.iir_lambda;  // lambda^TT (TT a power of two)
+  for (int s = 1; s < TT; s <<= 1) lamT = cmul(lamT, lamT);
+  V* tiles = as_t2<T>(d.raman_tiles) + (size_t)q * ntiles * 2;
+  Affine mine = affine_identity();
+  for (int i = first; i < last; ++i) {
+    mine.a = cmul(mine.a, lamT);
+    mine.ba = cadd(cmul(lamT, mine.ba), to_d2(tiles[2 * i]));
+    mine.bb = cadd(cmul(lamT, mine.bb), to_d2(tiles[2 * i + 1]));
+  }
+  const Affine incl = warp_scan_affine(mine, lane);
+  Affine pre = shfl_up_affine(incl, 1, 0xffffffffu);
+  if (lane == 0) pre = affine_identity();
+  const Affine tot = [&] {
+    Affine t;
+    t.a = make_double2(__shfl_sync(0xffffffffu, incl.a.x, 31), __shfl_sync(0xffffffffu, incl.a.y, 31));
+    t.ba = make_double2(__shfl_sync(0xffffffffu, incl.ba.x, 31), __shfl_sync(0xffffffffu, incl.ba.y, 31));
+    t.bb = make_double2(__shfl_sync(0xffffffffu, incl.bb.x, 31), __shfl_sync(0xffffffffu, incl.bb.y, 31));
+    return t;
+  }();
+  const double2 inv = d.iir_inv_one_minus;
+  double2 ca = cadd(cmul(pre.a, cmul(tot.ba, inv)), pre.ba);
+  double2 cb = cadd(cmul(pre.a, cmul(tot.bb, inv)), pre.bb);
+  for (int i = first; i < last; ++i) {
+    const double2 ga = to_d2(tiles[2 * i]), gb = to_d2(tiles[2 * i + 1]);
+    tiles[2 * i] = from_d2<T>(ca);
+    tiles[2 * i + 1] = from_d2<T>(cb);
+    ca = cadd(cmul(lamT, ca), ga);
+    cb = cadd(cmul(lamT, cb), gb);
+  }
+}
+
 // ---- k_contract: sigma_p(t) = sum_terms Q U_k(t) W(t) over a tile of t, all p ----------
 // The U tile [M][TT] and the R tile [P][TT] (Raman on) arrive in shared memory as
 // one bulk-async copy per row segment (TT contiguous samples), issued by the
@@ -799,9 +980,11 @@ template <typename T> struct StagedTerm {
   T q;
 };
 
+// raman_mode: 0 Raman off; 1 the convolutions R arrive as rows (k_pair / k_raman_scan);
+// 2 the recurrence runs through the tile here from the carries of k_raman_carry.
 template <typename T>
 __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
-                                                  int stage_terms) {
+                                                  int stage_terms, int raman_mode) {
   using V = c2<T>;
   using ST = StagedTerm<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -811,13 +994,14 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   const int t0 = blockIdx.x * TT;
   if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;  // empty slot / finished
   const int M = d.M;
-  const int raman = d.raman;
-  const int P = d.P;                  // pair fields formed in this tile
-  const int Pl = raman ? P : 0;       // pair rows loaded (Raman convolutions)
+  const int raman = raman_mode;
+  const int P = d.P;                          // pair fields formed in this tile
+  const int Pl = raman == 1 ? P : 0;          // pair rows loaded (Raman convolutions)
   const T kerr = (T)d.one_minus_fR;
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
-  ST* st = reinterpret_cast<ST*>(sU + (size_t)(M + P) * TT);
+  const size_t scratch = raman == 2 ? (size_t)(blockDim.x >> 5) * padded_len(TT) : 0;
+  ST* st = reinterpret_cast<ST*>(sU + (size_t)(M + P) * TT + scratch);
   if (stage_terms) {
     for (int j = threadIdx.x; j < n_terms; j += blockDim.x) {
       const Term tm = d.terms[j];
@@ -850,21 +1034,69 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
     return;
   }
   const int H = TT >> 1;  // sample pairs per row
-  // 1. pair fields, two samples per thread
-  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
-    const int q = idx / H, tt = 2 * (idx - q * H);
-    const int2 lm = d.pairs[q];
-    V ul0, ul1, um0, um1;
-    ld2<T>(sU + lm.x * TT + tt, ul0, ul1);
-    ld2<T>(sU + lm.y * TT + tt, um0, um1);
-    V w0 = cmulc(ul0, um0), w1 = cmulc(ul1, um1);
-    if (raman) {
-      V r0, r1;
-      ld2<T>(sW + q * TT + tt, r0, r1);
-      w0 = mk<T>(fma(kerr, w0.x, r0.x), fma(kerr, w0.y, r0.y));
-      w1 = mk<T>(fma(kerr, w1.x, r1.x), fma(kerr, w1.y, r1.y));
+  // 1. pair fields
+  if (raman != 2) {  // two samples per thread
+    for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+      const int q = idx / H, tt = 2 * (idx - q * H);
+      const int2 lm = d.pairs[q];
+      V ul0, ul1, um0, um1;
+      ld2<T>(sU + lm.x * TT + tt, ul0, ul1);
+      ld2<T>(sU + lm.y * TT + tt, um0, um1);
+      V w0 = cmulc(ul0, um0), w1 = cmulc(ul1, um1);
+      if (raman) {
+        V r0, r1;
+        ld2<T>(sW + q * TT + tt, r0, r1);
+        w0 = mk<T>(fma(kerr, w0.x, r0.x), fma(kerr, w0.y, r0.y));
+        w1 = mk<T>(fma(kerr, w1.x, r1.x), fma(kerr, w1.y, r1.y));
+      }
+      st2<T>(sW + q * TT + tt, w0, w1);
     }
-    st2<T>(sW + q * TT + tt, w0, w1);
+  } else {  // one warp per pair field: the recurrence through the tile, then W
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    V* scr = sW + (size_t)P * TT + (size_t)warp * padded_len(TT);
+    TileScan<T> ts;
+    ts.init(d, TT >> 5, lane);
+    const int ntiles = nt / TT;
+    const V* tiles = as_t2<T>(d.raman_tiles);
+    for (int q = warp; q < P; q += nwarps) {
+      ts.form(sU, TT, d.pairs[q], scr, lane);
+      __syncwarp();
+      V la, lb;
+      ts.lane_local(scr, lane, la, lb);
+      ts.lane_scan(la, lb, lane);
+      // state entering this lane's samples: lambda^(c lane) C_tile + earlier lanes
+      V ea, eb;
+      ea.x = __shfl_up_sync(0xffffffffu, la.x, 1);
+      ea.y = __shfl_up_sync(0xffffffffu, la.y, 1);
+      eb.x = __shfl_up_sync(0xffffffffu, lb.x, 1);
+      eb.y = __shfl_up_sync(0xffffffffu, lb.y, 1);
+      if (lane == 0) ea = eb = mk<T>(0, 0);
+      const size_t ti = ((size_t)q * ntiles + blockIdx.x) * 2;
+      const V Ca = cadd(cmul(ts.lane_pow, tiles[ti]), ea);
+      const V Cb = cadd(cmul(ts.lane_pow, tiles[ti + 1]), eb);
+      const V kca = cmul(ts.kt, Ca), kcb = cmul(ts.kt, Cb);
+      la = mk<T>(0, 0);
+      lb = mk<T>(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k < ts.c) {
+          V& cell = scr[pad(ts.c * lane + k)];
+          const V x = cell;
+          la = ts.step(la, x.x);
+          lb = ts.step(lb, x.y);
+          // R = Im(kappa local) + Im(lambda^(k+1) kappa C), W = (1 - f_R) V + R
+          const T rx = fma(ts.kt.x, la.y, fma(ts.kt.y, la.x, fma(ts.pw[k].x, kca.y, ts.pw[k].y * kca.x)));
+          const T ry = fma(ts.kt.x, lb.y, fma(ts.kt.y, lb.x, fma(ts.pw[k].x, kcb.y, ts.pw[k].y * kcb.x)));
+          cell = mk<T>(fma(kerr, x.x, rx), fma(kerr, x.y, ry));
+        }
+      }
+      __syncwarp();
+      for (int j = 0; j < ts.c; ++j) {
+        const int e = 32 * j + lane;
+        sW[q * TT + e] = scr[pad(e)];
+      }
+      __syncwarp();
+    }
   }
   __syncthreads();
   // 2. contraction

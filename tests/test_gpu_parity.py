@@ -187,10 +187,14 @@ def test_raman_recurrence_matches_fft_convolution(mmp, monkeypatch, fp64, nt, wi
     # path on the same solve and against the oracle
     prob = W.small_case(seed=91, M=3, nt=nt, n_steps=6, window=window, nnz_target=10)
     fl = capi.MMP_F_FP64 if fp64 else 0
-    out_r, info_r = run(mmp, prob, [6], fl)
+    out_r, info_r = run(mmp, prob, [6], fl)            # inside the contraction tiles
+    monkeypatch.setenv("MMP_RAMAN_FUSED", "0")
+    out_s, info_s = run(mmp, prob, [6], fl)            # row scan
     monkeypatch.setenv("MMP_RAMAN_FFT", "1")
-    out_f, info_f = run(mmp, prob, [6], fl)
-    assert (info_r["raman_recurrence"], info_f["raman_recurrence"]) == (1, 0)
-    assert mo.rel_l2_per_mode(out_r, out_f).max() < (1e-12 if fp64 else 2e-6)
+    out_f, info_f = run(mmp, prob, [6], fl)            # FFT convolution
+    assert (info_r["raman_recurrence"], info_s["raman_recurrence"], info_f["raman_recurrence"]) == (2, 1, 0)
+    tol = 1e-12 if fp64 else 2e-6
+    assert mo.rel_l2_per_mode(out_r, out_f).max() < tol
+    assert mo.rel_l2_per_mode(out_s, out_f).max() < tol
     ref = mo.solve(prob)
     assert mo.rel_l2_per_mode(out_r, ref).max() < (TOL64 if fp64 else TOL32)
