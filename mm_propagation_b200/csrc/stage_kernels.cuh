@@ -49,20 +49,37 @@ __device__ __forceinline__ double alpha_of(int k, int nt, double alpha_scale) {
   return alpha_scale * (double)kk;
 }
 
-// exp(i theta): theta reduced mod 2 pi in FP64 (Cody–Waite with a two-part
-// 2 pi), then sincos in precision T.
+// exp(i theta) with theta reduced in FP64 (Cody–Waite with a two-part constant).
+// FP32: reduced by pi/2 to x in [-pi/4, pi/4] and quadrant n mod 4, then the Taylor
+// series of sin and cos to x^9 and x^10 (truncation below 2e-9 on that interval),
+// evaluated by Horner in x^2 in FP32; the quadrant swaps and negates. Short, branch-free
+// code with no large-argument path (the argument is already small). FP64: reduced by
+// 2 pi, then sincos.
 template <typename T> __device__ __forceinline__ c2<T> expi(double theta) {
-  constexpr double kInv2Pi = 0.15915494309189533577;
-  constexpr double kTwoPiHi = 6.28318530717958623200;   // nearest double to 2 pi
-  constexpr double kTwoPiLo = 2.4492935982947063697e-16;  // 2 pi - kTwoPiHi
-  const double n = rint(theta * kInv2Pi);
-  double r = fma(-n, kTwoPiHi, theta);
-  r = fma(-n, kTwoPiLo, r);
   if constexpr (sizeof(T) == 4) {
-    float s, c;
-    sincosf((float)r, &s, &c);
-    return make_float2(c, s);
+    constexpr double k2OverPi = 0.63661977236758134308;
+    constexpr double kHalfPiHi = 1.57079632679489655800;    // nearest double to pi/2
+    constexpr double kHalfPiLo = 6.12323399573676603587e-17;  // pi/2 - kHalfPiHi
+    const double n = rint(theta * k2OverPi);
+    const double r = fma(-n, kHalfPiLo, fma(-n, kHalfPiHi, theta));
+    const float x = (float)r, x2 = x * x;
+    // sin x = x (1 - x^2/3! + x^4/5! - x^6/7! + x^8/9!), cos x = 1 - x^2/2! + ... - x^10/10!
+    const float sp =
+        x * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f), -1.0f / 6.0f), 1.0f);
+    const float cp = fmaf(
+        x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -1.0f / 3628800.0f, 1.0f / 40320.0f), -1.0f / 720.0f), 1.0f / 24.0f),
+                 -0.5f),
+        1.0f);
+    const int q = (int)(long long)n & 3;
+    const float c = (q & 1) ? sp : cp, s = (q & 1) ? cp : sp;
+    return make_float2((q == 1 || q == 2) ? -c : c, (q >= 2) ? -s : s);
   } else {
+    constexpr double kInv2Pi = 0.15915494309189533577;
+    constexpr double kTwoPiHi = 6.28318530717958623200;   // nearest double to 2 pi
+    constexpr double kTwoPiLo = 2.4492935982947063697e-16;  // 2 pi - kTwoPiHi
+    const double n = rint(theta * kInv2Pi);
+    double r = fma(-n, kTwoPiHi, theta);
+    r = fma(-n, kTwoPiLo, r);
     double s, c;
     sincos(r, &s, &c);
     return make_double2(c, s);
