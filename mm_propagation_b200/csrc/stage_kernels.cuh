@@ -484,8 +484,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // Stage-combination list: the stored N_hat_j entering x_hat (or, at the last stage,
   // psi_{n+1} = psi_n + h sum_j b_j N_j, src/MultimodePropagation_CPU.cpp:75-85) with
   // their coefficients h*a or h*b; N_hat_i itself comes from registers (cself).
-  // Thread 0 also starts L2 prefetches of the psi_hat and N_hat_j spans this CTA
-  // reads after its forward transform, so they arrive while the transform runs.
+  // Once its sigma loads are issued, thread 0 starts L2 prefetches of the psi_hat and
+  // N_hat_j spans this CTA reads after its forward transform, so they arrive while the
+  // transform runs.
   __shared__ int s_jq[kMaxStages];
   __shared__ double s_cq[kMaxStages];
   __shared__ int s_nq;
@@ -511,11 +512,6 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         if (kp.tab.a[i + 1][j] != 0.0) { s_jq[nq] = j; s_cq[nq] = kp.tab.a[i + 1][j] * h; ++nq; }
     }
     s_nq = nq;
-    for (int qb = 0; qb < Gm::C; ++qb) {  // the CTA's frequencies: C spans of CH
-      const size_t f0 = row + (size_t)rank * Gm::CH + (size_t)Gm::NL * qb;
-      prefetch_l2(d.psi_hat + f0, Gm::CH * (unsigned)sizeof(double2));
-      for (int q = 0; q < nq; ++q) prefetch_l2(Nh + (size_t)s_jq[q] * mstride + f0, Gm::CH * (unsigned)sizeof(V));
-    }
   }
   const V* sig = as_t2<T>(d.sigma);
   if constexpr (Gm::C == 1 && sizeof(T) == 4) {
@@ -529,6 +525,16 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   } else {
 #pragma unroll 8
     for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = sig[(size_t)p * Gm::N + Gm::time_of(rank, u)];
+  }
+  if (tid == 0) {  // after this thread's sigma loads, so the prefetches do not delay them
+    const size_t prow = (size_t)p * Gm::N;
+    const size_t pstride = (size_t)d.M * Gm::N;
+    const V* Nq = as_t2<T>(d.Nh);
+    for (int qb = 0; qb < Gm::C; ++qb) {  // the CTA's frequencies: C spans of CH
+      const size_t f0 = prow + (size_t)rank * Gm::CH + (size_t)Gm::NL * qb;
+      prefetch_l2(d.psi_hat + f0, Gm::CH * (unsigned)sizeof(double2));
+      for (int q = 0; q < s_nq; ++q) prefetch_l2(Nq + (size_t)s_jq[q] * pstride + f0, Gm::CH * (unsigned)sizeof(V));
+    }
   }
   forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers also publish the values thread 0 wrote
   const int i = kp.stage;
