@@ -152,13 +152,22 @@ def make_batch_problems(args, rank: int):
             for i in range(args.batch)]
 
 
-def stage_bytes(prob, tab_s, a, b, bt, pairs):
+def stage_bytes(prob, tab_s, a, b, bt, pairs, raman_path):
     """Algorithmic DRAM bytes per launch for each kernel kind, one solve, averaged
-    over the stages of a step (complex elements of bt bytes; psi_hat is FP64)."""
+    over the stages of a step (complex elements of bt bytes; psi_hat is FP64).
+    raman_path (mmp_info.raman_recurrence): 0 pair fields by FFT convolution (k_pair),
+    1 by the row recurrence (k_raman_scan), 2 by the recurrence inside the contraction
+    tiles (k_raman_agg + k_raman_carry; their per-tile carries, under 1% of the bytes,
+    are not counted)."""
     M, NT = prob.n_modes, prob.nt
-    P = pairs
-    pair = (M + P + 1) * NT * bt                       # read U, write W, read H_R
-    contract = (2 * M + P) * NT * bt                   # read U and W, write sigma
+    P = pairs if prob.raman else 0
+    if raman_path == 0:
+        pair = (M + P + 1) * NT * bt                   # read U, write R, read H_R
+    elif raman_path == 1:
+        pair = (M + P) * NT * bt                       # read U, write R
+    else:
+        pair = M * NT * bt                             # read U
+    contract = (2 * M + (P if raman_path in (0, 1) else 0)) * NT * bt  # read U (and R), write sigma
     nu = 0.0
     for i in range(tab_s):
         last = i == tab_s - 1
@@ -169,6 +178,34 @@ def stage_bytes(prob, tab_s, a, b, bt, pairs):
             rows += sum(1 for j in range(i) if a[i + 1][j] != 0) * M * bt  # N_i is in registers
         nu += rows * NT
     return {"pair": pair, "contract": contract, "nu": nu / tab_s}
+
+
+def stage_flops(prob, pairs, n_terms, raman_path):
+    """Algorithmic FP32 flops per launch for each kernel kind, one solve: 5 N log2 N per
+    complex transform; the recurrence 24 flops per sample and pair field (two complex
+    first-order scans, output and pair product); 8 per contraction term and sample;
+    about 70 per sample for k_nu's phase factors and stage combination."""
+    M, NT = prob.n_modes, prob.nt
+    P = pairs if prob.raman else 0
+    fft = 5.0 * NT * math.log2(NT)
+    if raman_path == 0:
+        pair = P * (2 * fft + 12 * NT)
+    else:
+        pair = P * NT * 24.0
+    contract = NT * (8.0 * n_terms + 6.0 * P)
+    nu = M * (2 * fft + 70.0 * NT)
+    return {"pair": pair, "contract": contract, "nu": nu}
+
+
+def fp32_peak_tflops():
+    """Nominal FP32 (non-tensor) peak: 148 SMs x 128 lanes x 2 flops x max SM clock.
+    MEASURED_PEAKS.json carries no FP32 figure."""
+    mhz = 1965.0
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", mhz))
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
 
 
 def read_measured_peaks():
@@ -319,25 +356,40 @@ def ours_arm(args, dist):
     # roofline of the dominant kernel
     bt = 16 if args.fp64 else 8
     tab = batch_tableau(args.order)
-    per = stage_bytes(probe, tab[3], tab[0], tab[1], bt, n_pairs)
+    raman_path = info["raman_recurrence"]
+    n_terms = int((probe.coupling["value"] != 0).sum())
+    per = stage_bytes(probe, tab[3], tab[0], tab[1], bt, n_pairs, raman_path)
+    flops = stage_flops(probe, n_pairs, n_terms, raman_path)
+    names = {"pair": ("k_pair", "k_raman_scan", "k_raman_agg+k_raman_carry")[raman_path],
+             "contract": "k_contract", "nu": "k_nu"}
     share = {k: prof[k]["ms_per_launch"] * prof[k]["launches"] for k in prof}
     tot = sum(share.values())
     dom = max(share, key=share.get)
     peak, peak_kind = read_measured_peaks()
+    fpeak = fp32_peak_tflops()
     kernels = {}
     for k in prof:
         if not prof[k]["launches"]:
             continue
+        t = prof[k]["ms_per_launch"] / 1e3
         bytes_launch = per[k] * args.batch
-        ach = bytes_launch / (prof[k]["ms_per_launch"] / 1e3) / 1e9
-        kernels[k] = {"ms_per_launch": prof[k]["ms_per_launch"], "share": share[k] / tot,
-                      "alg_bytes_per_launch": bytes_launch, "achieved_gbs": ach, "frac": ach / peak}
-    traffic_solve = read_ncu_traffic({"pair": "k_pair", "contract": "k_contract", "nu": "k_nu"}[dom], "grin6")
-    roof = {"bound": "hbm", "kernel": {"pair": "k_pair", "contract": "k_contract", "nu": "k_nu"}[dom],
+        flops_launch = flops[k] * args.batch
+        ach = bytes_launch / t / 1e9
+        t_hbm, t_fp32 = bytes_launch / (peak * 1e9), flops_launch / (fpeak * 1e12)
+        kernels[k] = {"name": names[k], "ms_per_launch": prof[k]["ms_per_launch"], "share": share[k] / tot,
+                      "alg_bytes_per_launch": bytes_launch, "achieved_gbs": ach, "frac": ach / peak,
+                      "alg_flops_per_launch": flops_launch, "achieved_tflops": flops_launch / t / 1e12,
+                      "fp32_frac": flops_launch / t / 1e12 / fpeak,
+                      "roofline_bound": "hbm" if t_hbm >= t_fp32 else "fp32",
+                      "roofline_frac": max(t_hbm, t_fp32) / t}
+    traffic_solve = read_ncu_traffic(names[dom].split("+")[0], "grin6")
+    roof = {"bound": "hbm", "kernel": names[dom],
             "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
             "frac": kernels[dom]["frac"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic_solve * args.batch if traffic_solve else None,
-            "alg_bytes_per_launch": kernels[dom]["alg_bytes_per_launch"], "kernels": kernels}
+            "alg_bytes_per_launch": kernels[dom]["alg_bytes_per_launch"],
+            "fp32_peak_tflops": fpeak, "fp32_peak_source": "nominal: 148 SMs x 128 lanes x 2 x max SM clock",
+            "kernels": kernels}
 
     # accuracy and the CPU baseline (rank 0, N=1 only)
     cpu = None
