@@ -11,6 +11,9 @@ mode power splits and phases) advanced by the same launches. One bench step is
 R Lawson–RK steps of the whole batch. value = all ranks' B*M*NT*R*K / device
 time (CUDA events on the solver's stream, max over ranks).
 
+--workload grin2 | dense15 | sweep28 measures the other configurations the same way
+(see WORKLOADS and make_problem); --workload serve the mixed request stream.
+
 The peak power is set where the reference's own FP64 solver is stable and
 converged at this step size (see workloads.grin6 and the accuracy block); the
 throughput per step does not depend on it.
@@ -44,21 +47,36 @@ def parse():
     ap.add_argument("--steps", type=int, default=40, help="timed bench steps (each R RK steps)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--batch", type=int, default=32, help="independent solves per GPU")
-    ap.add_argument("--rk-per-step", type=int, default=50, help="RK steps per bench step")
-    ap.add_argument("--order", type=int, default=4)
-    ap.add_argument("--peak-w", type=float, default=10.0, help="total peak power per solve (W)")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS) + ("serve",), default="grin6",
+                    help="grin6: the batched 6-mode step (default); grin2, dense15, sweep28: the "
+                         "other configurations; serve: the mixed request stream")
+    ap.add_argument("--batch", type=int, default=None, help="independent solves per GPU")
+    ap.add_argument("--rk-per-step", type=int, default=None, help="RK steps per bench step")
+    ap.add_argument("--order", type=int, default=4, help="RK order (grin6)")
+    ap.add_argument("--peak-w", type=float, default=None, help="grin6: total peak power per solve (W)")
     ap.add_argument("--fp64", action="store_true", help="all-FP64 arithmetic")
     ap.add_argument("--e2e-iters", type=int, default=2)
-    ap.add_argument("--cpu-steps", type=int, default=6, help="RK steps per process in the CPU sample")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="RK steps of an e2e solve (default per workload)")
+    ap.add_argument("--cpu-steps", type=int, default=None, help="RK steps per process in the CPU sample")
+    ap.add_argument("--acc-steps", type=int, default=None, help="RK steps of the FP32-vs-FP64 check")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
-    ap.add_argument("--workload", choices=("grin6", "serve"), default="grin6",
-                    help="grin6: the batched 6-mode step (default); serve: the mixed request stream")
     ap.add_argument("--requests", type=int, default=512, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean Poisson arrival rate (1/s)")
     ap.add_argument("--check", type=int, default=4, help="serve: requests re-solved in FP64 for relL2")
-    return ap.parse_args()
+    args = ap.parse_args()
+    w = WORKLOADS.get(args.workload, WORKLOADS["grin6"])
+    if args.batch is None:
+        args.batch = w["batch"]
+    if args.rk_per_step is None:
+        args.rk_per_step = w["rk"]
+    if args.e2e_steps is None:
+        args.e2e_steps = w["e2e"]
+    if args.cpu_steps is None:
+        args.cpu_steps = w["cpu"]
+    if args.acc_steps is None:
+        args.acc_steps = w["acc"]
+    return args
 
 
 # ---- process-group plumbing ----------------------------------------------------------------
@@ -145,10 +163,47 @@ class Clocks:
 
 
 # ---- workload ------------------------------------------------------------------------------
+# Per workload: batch per GPU, RK steps per bench step, RK steps of an e2e solve (None:
+# the full n_steps), RK steps of the CPU sample, RK steps of the FP32-vs-FP64 check
+# (None: full solve, plus FP64 at 2x steps).
+WORKLOADS = {
+    "grin6": dict(batch=32, rk=50, e2e=None, cpu=6, acc=None,
+                  desc="grin6: M=6, NT=16384, 20 ps, 1 m, 5000 steps, GRIN Q, Raman on"),
+    "grin2": dict(batch=128, rk=100, e2e=None, cpu=20, acc=None,
+                  desc="grin2: M=2, NT=4096, 10 ps, 0.1 m, 1000 steps, the four-entry pattern, Raman on"),
+    "dense15": dict(batch=16, rk=10, e2e=400, cpu=2, acc=200,
+                    desc="dense15: M=15, NT=8192, 20 ps, 0.5 m, 4000 steps, dense symmetric Q (50625 terms), Raman on"),
+    "sweep28": dict(batch=32, rk=4, e2e=100, cpu=1, acc=100,
+                    desc="sweep28: M=28, NT=65536, 20 ps, 2 m, 10000 steps, order 6, ~2000 GRIN terms, Raman on, "
+                         "peaks log-spaced over the batch"),
+}
+
+
+def make_problem(workload: str, seed: int, order: int, peak_w, flags: int = 0):
+    """One member of a workload (module level: the CPU worker processes build theirs
+    the same way). Power levels: grin6 at `peak_w` total (default 10 W); grin2 at 1/100
+    of the stated 10 kW / 1 kW; dense15 and sweep28 at the stated powers lowered by one
+    factor (for sweep28 the top of the ladder's) until the nonlinear phase is at most
+    5.6e-3 rad per step and 28 rad per fiber, the 6-mode workload's levels at 10 W:
+    at the stated powers RK4/RK6 at these step lengths diverge."""
+    from mm_propagation_b200 import workloads as W
+    if workload == "grin6":
+        return W.grin6(seed=seed, order=order, peak_total_w=10.0 if peak_w is None else peak_w, flags=flags)
+    if workload == "grin2":
+        return W.grin2(seed=seed, peak_scale=0.01, flags=flags)
+    if workload == "dense15":
+        p = W.dense15(seed=seed, flags=flags)
+        return W.scale_power(p, W.phase_cap_scale(p))
+    if workload == "sweep28":
+        top = W.sweep28(seed=0, index=31)
+        return W.scale_power(W.sweep28(seed=0, index=seed % 32, flags=flags), W.phase_cap_scale(top))
+    raise ValueError(workload)
+
+
 def make_batch_problems(args, rank: int):
-    from mm_propagation_b200 import capi, workloads as W
+    from mm_propagation_b200 import capi
     flags = capi.MMP_F_FP64 if args.fp64 else 0
-    return [W.grin6(seed=1000 * rank + i, order=args.order, peak_total_w=args.peak_w, flags=flags)
+    return [make_problem(args.workload, 1000 * rank + i, args.order, args.peak_w, flags)
             for i in range(args.batch)]
 
 
@@ -234,13 +289,12 @@ def _ref_worker(q, spec):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np  # noqa: F401
     import ref_lib
-    from mm_propagation_b200 import workloads as W
-    prob = W.grin6(seed=spec["seed"], order=spec["order"], peak_total_w=spec["peak_w"])
+    prob = make_problem(spec["workload"], spec["seed"], spec["order"], spec["peak_w"])
     out, sec = ref_lib.run(prob, [spec["steps"]])
     q.put((spec["index"], sec, out if spec["keep"] else None, ref_lib.threads(prob.n_modes)))
 
 
-def run_reference_cpu(n_members: int, steps: int, order: int, peak_w: float, keep_first: bool):
+def run_reference_cpu(workload: str, n_members: int, steps: int, order: int, peak_w, keep_first: bool):
     ncpu = os.cpu_count() or 1
     nproc = max(1, min(n_members, ncpu))
     threads = max(1, ncpu // nproc)
@@ -248,7 +302,7 @@ def run_reference_cpu(n_members: int, steps: int, order: int, peak_w: float, kee
     q = ctx.Queue()
     procs = []
     for i in range(nproc):
-        spec = {"seed": i, "order": order, "peak_w": peak_w, "steps": steps, "threads": threads,
+        spec = {"workload": workload, "seed": i, "order": order, "peak_w": peak_w, "steps": steps, "threads": threads,
                 "index": i, "keep": keep_first and i == 0}
         p = ctx.Process(target=_ref_worker, args=(q, spec))
         p.start()
@@ -266,10 +320,9 @@ def run_reference_cpu(n_members: int, steps: int, order: int, peak_w: float, kee
 def reference_arm(args, dist):
     if dist.rank != 0:
         return None
-    from mm_propagation_b200 import workloads as W
-    probe = W.grin6(seed=0, order=args.order, peak_total_w=args.peak_w)
-    steps = max(1, min(args.steps, 20))
-    r = run_reference_cpu(args.batch, steps, args.order, args.peak_w, keep_first=False)
+    probe = make_problem(args.workload, 0, args.order, args.peak_w)
+    steps = max(1, min(args.steps, 20 if args.workload in ("grin6", "grin2") else 2))
+    r = run_reference_cpu(args.workload, args.batch, steps, args.order, args.peak_w, keep_first=False)
     work = r["procs"] * probe.n_modes * probe.nt * steps
     value = work / r["max_seconds"]
     cores = r["procs"] * r["effective_omp_threads"]
@@ -290,12 +343,13 @@ def reference_arm(args, dist):
 
 
 def workload_config(args, probe, world):
-    from mm_propagation_b200 import capi  # noqa: F401
     nnz = int((probe.coupling["value"] != 0).sum())
-    return {"workload": f"grin6: M={probe.n_modes}, NT={probe.nt}, RK order {args.order}, Raman on, "
-                        f"{nnz} GRIN non-zeros, batch of {args.batch} independent solves per GPU",
+    return {"workload": f"{WORKLOADS[args.workload]['desc']}; M={probe.n_modes}, NT={probe.nt}, "
+                        f"RK order {probe.method_order}, {nnz} non-zero Q entries; batch of {args.batch} "
+                        f"independent solves per GPU",
             "global_batch": args.batch * world, "rk_steps_per_bench_step": args.rk_per_step,
-            "peak_total_w": args.peak_w, "precision": "fp64" if args.fp64 else "fp32-bulk+fp64-phase/accum",
+            "peak_total_w": probe.notes.get("peak_total_w"), "power_scale": probe.notes.get("power_scale", 1.0),
+            "precision": "fp64" if args.fp64 else "fp32-bulk+fp64-phase/accum",
             "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (batch state > 126 MB)"}
 
 
@@ -340,7 +394,7 @@ def ours_arm(args, dist):
     import torch
     pin_in = [torch.from_numpy(np.ascontiguousarray(p.initial_fields)).pin_memory() for p in probs]
     pin_out = [torch.empty((p.n_modes, p.nt), dtype=torch.complex128).pin_memory() for p in probs]
-    nsteps = probe.n_steps
+    nsteps = probe.n_steps if args.e2e_steps is None else min(args.e2e_steps, probe.n_steps)
     dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_iters):
@@ -382,7 +436,7 @@ def ours_arm(args, dist):
                       "fp32_frac": flops_launch / t / 1e12 / fpeak,
                       "roofline_bound": "hbm" if t_hbm >= t_fp32 else "fp32",
                       "roofline_frac": max(t_hbm, t_fp32) / t}
-    traffic_solve = read_ncu_traffic(names[dom].split("+")[0], "grin6")
+    traffic_solve = read_ncu_traffic(names[dom].split("+")[0], args.workload)
     roof = {"bound": "hbm", "kernel": names[dom],
             "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
             "frac": kernels[dom]["frac"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -396,14 +450,13 @@ def ours_arm(args, dist):
     acc = None
     if dist.rank == 0 and dist.world == 1 and not args.no_accuracy:
         cs = args.cpu_steps
-        r = run_reference_cpu(args.batch, cs, args.order, args.peak_w, keep_first=True)
+        r = run_reference_cpu(args.workload, args.batch, cs, args.order, args.peak_w, keep_first=True)
         cpu_value = r["procs"] * M * NT * cs / r["max_seconds"]
         cpu = {"value": cpu_value, "unit": METRIC, "cores": r["procs"] * r["effective_omp_threads"],
                "kind": "reference",
                "sample": f"{r['procs']} concurrent reference solves of this workload (oracle/_ref, "
                          f"unmodified reference sources + FFTW-API shim), {cs} RK steps each"}
-        from mm_propagation_b200 import workloads as W
-        p0 = W.grin6(seed=0, order=args.order, peak_total_w=args.peak_w)
+        p0 = make_problem(args.workload, 0, args.order, args.peak_w)
         acc = {}
         for name, fl in (("fp32", 0), ("fp64", capi.MMP_F_FP64)):
             with mmp.Solver(p0.replace(flags=fl)) as s:
@@ -412,19 +465,23 @@ def ours_arm(args, dist):
             ref = r["first_output"]
             err = np.sqrt((np.abs(out - ref) ** 2).sum(-1) / (np.abs(ref) ** 2).sum(-1)).max()
             acc[f"relL2_max_{name}_vs_reference_{cs}_steps"] = float(err)
-        full = {}
-        for name, fl in (("fp32", 0), ("fp64", capi.MMP_F_FP64)):
-            with mmp.Solver(p0.replace(flags=fl)) as s:
-                s.propagate(p0.n_steps)
-                full[name] = s.result()
-        with mmp.Solver(p0.replace(flags=capi.MMP_F_FP64, n_steps=2 * p0.n_steps)) as s:
-            s.propagate(2 * p0.n_steps)
-            full["fp64_2x"] = s.result()
 
         def rel(x, y):
             return float(np.sqrt((np.abs(x - y) ** 2).sum(-1) / (np.abs(y) ** 2).sum(-1)).max())
-        acc["relL2_max_fp32_vs_fp64_full_solve"] = rel(full["fp32"], full["fp64"])
-        acc["relL2_max_fp64_vs_fp64_2x_steps_full_solve"] = rel(full["fp64"], full["fp64_2x"])
+        na = p0.n_steps if args.acc_steps is None else min(args.acc_steps, p0.n_steps)
+        full = {}
+        for name, fl in (("fp32", 0), ("fp64", capi.MMP_F_FP64)):
+            with mmp.Solver(p0.replace(flags=fl)) as s:
+                s.propagate(na)
+                full[name] = s.result()
+        if na == p0.n_steps:
+            with mmp.Solver(p0.replace(flags=capi.MMP_F_FP64, n_steps=2 * p0.n_steps)) as s:
+                s.propagate(2 * p0.n_steps)
+                full["fp64_2x"] = s.result()
+            acc["relL2_max_fp32_vs_fp64_full_solve"] = rel(full["fp32"], full["fp64"])
+            acc["relL2_max_fp64_vs_fp64_2x_steps_full_solve"] = rel(full["fp64"], full["fp64_2x"])
+        else:
+            acc[f"relL2_max_fp32_vs_fp64_{na}_steps"] = rel(full["fp32"], full["fp64"])
         acc["tolerance"] = 1e-5
     batch.close()
     line = {

@@ -415,6 +415,26 @@ def stream(seed: int = 0, n: int = 512, rate_hz: float = 200.0, median_peak_w: f
     return out
 
 
+def phase_cap_scale(prob: Problem, per_step: float = STREAM_PHASE_CAP,
+                    total: float = STREAM_TOTAL_PHASE_CAP) -> float:
+    """Power factor (<= 1) that brings prob's nonlinear phase to at most `per_step` rad
+    per step and `total` rad over the fiber (the 6-mode workload's levels at 10 W,
+    where the solve is converged and FP32 bulk meets relL2 <= 1e-5)."""
+    f = nonlinear_phase_per_step(prob)
+    if f <= 0:
+        return 1.0
+    return min(1.0, per_step / f, total / (f * prob.n_steps))
+
+
+def scale_power(prob: Problem, factor: float) -> Problem:
+    """prob with every initial field's power multiplied by `factor`."""
+    notes = dict(prob.notes)
+    notes["power_scale"] = factor
+    if "peak_total_w" in notes:
+        notes["peak_total_w"] = notes["peak_total_w"] * factor
+    return prob.replace(initial_fields=prob.initial_fields * math.sqrt(factor), notes=notes)
+
+
 def small_case(seed: int = 0, M: int = 2, nt: int = 256, n_steps: int = 20, order: int = 4,
                raman: bool = True, window: float = 10.0, fiber_length: float = 0.01,
                peak_w: float = 200.0, nnz_target: int = 12, physical_order: bool = False,
