@@ -109,6 +109,8 @@ typedef struct mmp_info {
                                                a damped sinusoid h_i = Im(c lambda^i)) 1 in a row
                                                pass, 2 inside the contraction tiles */
   uint32_t graph_branches;                  /* independent solve groups per captured graph */
+  uint32_t dense_contraction;               /* 1: the contraction runs as a dense register-blocked
+                                               product over (p, k) x pair fields (M <= 16) */
 } mmp_info;
 
 typedef struct mmp_solver mmp_solver;

@@ -76,6 +76,7 @@ class mmp_info(C.Structure):
         ("cluster_ctas", C.c_uint32),
         ("raman_recurrence", C.c_uint32),
         ("graph_branches", C.c_uint32),
+        ("dense_contraction", C.c_uint32),
     ]
 
 

@@ -124,7 +124,14 @@ struct SolveDesc {
   // [P][NT/16][2] (T complex): per contraction tile and pair field, the recurrence's
   // tile aggregate (k_raman_agg), then the state entering the tile (k_raman_carry)
   void* raman_tiles;
+  // Dense form of the contraction (M <= kDenseMaxModes), T values [M][P][2 kDenseMaxModes]:
+  // entry (p, q, k) sums Q over the terms of p with U_k and pair field q, entry
+  // (p, q, kDenseMaxModes + k) the same with the sign of conj-read terms; null if unused
+  const void* dense_q;
 };
+
+// Largest mode count of the dense contraction form (its accumulators live in registers).
+constexpr int kDenseMaxModes = 16;
 
 // RK tableau passed by value to the stage kernels (identical for a batch).
 struct Tableau {

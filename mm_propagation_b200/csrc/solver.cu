@@ -155,10 +155,11 @@ int ensure_device(int dev, DeviceRes** out) {
         for (const void* f : fns)
           CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
       }
-  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<float>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract<double>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  const void* contract_fns[] = {(const void*)&k_contract<float, 0>,  (const void*)&k_contract<float, 1>,
+                                (const void*)&k_contract<float, 2>,  (const void*)&k_contract<double, 0>,
+                                (const void*)&k_contract<double, 1>, (const void*)&k_contract<double, 2>};
+  for (const void* f : contract_fns)
+    CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
@@ -293,6 +294,7 @@ struct Member {
   std::vector<int> term_off;
   std::vector<double> poly;
   bool quirk = false;
+  bool dense_ok = false;  // the dense contraction form is built for this solve
   uint32_t flags = 0;
   // device
   void* block = nullptr;  // one allocation for all per-solve buffers
@@ -475,6 +477,7 @@ struct mmp_batch {
   uint32_t groups = 1;
   bool raman_iir = false;  // every solve's h_R is a damped sinusoid: pair fields by k_raman_scan
   bool raman_fused = false;  // ... and the recurrence runs inside the contraction tiles
+  int dense = 0;  // contraction form: 0 term loop, 1 dense (k_contract<T, 1>), 2 per solve
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -565,7 +568,11 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   int mode = !b->raman ? 0 : (b->raman_fused ? 2 : 1);
   void* args[] = {(void*)&descs, &nt, &TT, &sterms, &mode};
   dim3 grid((unsigned)(b->nt / b->TT), count, 1);
-  const void* fn = b->fp64 ? (const void*)&k_contract<double> : (const void*)&k_contract<float>;
+  const void* f32[] = {(const void*)&k_contract<float, 0>, (const void*)&k_contract<float, 1>,
+                       (const void*)&k_contract<float, 2>};
+  const void* f64[] = {(const void*)&k_contract<double, 0>, (const void*)&k_contract<double, 1>,
+                       (const void*)&k_contract<double, 2>};
+  const void* fn = b->fp64 ? f64[b->dense] : f32[b->dense];
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, args));
   return MMP_OK;
 }
@@ -865,6 +872,16 @@ bool same_shape(const mmp_batch* b, const mmp_params* p) {
          std::memcmp(&t, &b->tab, sizeof(t)) == 0;
 }
 
+// Build the dense contraction form for this solve? When its term count is above half
+// the dense matrix's size (M^2 P) the register-blocked product does less work than the
+// term loop. MMP_DENSE=0 / 1 forces the choice (M <= 16 either way).
+bool dense_wanted(const mmp_batch* b, const Member& s) {
+  (void)b;
+  if (s.M > (uint32_t)kDenseMaxModes || s.pairs.empty()) return false;
+  if (const char* env = std::getenv("MMP_DENSE")) return std::atoi(env) == 1;
+  return 2 * s.terms.size() > (size_t)s.M * s.M * s.pairs.size();
+}
+
 size_t member_bytes(const mmp_batch* b, const Member& s) {
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
@@ -877,6 +894,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + (b->raman ? P : 0) * nt * t2);                           // W (R)
   off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));    // H
   off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);                // Raman tile carries
+  off = align_up(off + (dense_wanted(b, s) ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));  // dense form
   off = align_up(off + s.poly.size() * sizeof(double));
   off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -936,6 +954,8 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
   const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
   const size_t o_rt = off; off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);
+  s.dense_ok = dense_wanted(b, s);
+  const size_t o_dq = off; off = align_up(off + (s.dense_ok ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));
   const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
   const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -973,6 +993,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.W = T2ptr(s.block, o_w);
   d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
   d.raman_tiles = b->raman ? T2ptr(s.block, o_rt) : nullptr;
+  d.dense_q = s.dense_ok ? T2ptr(s.block, o_dq) : nullptr;
   d.pairs = (const int2*)T2ptr(s.block, o_pairs);
   d.terms = (const Term*)T2ptr(s.block, o_terms);
   d.term_off = (const int*)T2ptr(s.block, o_toff);
@@ -1001,6 +1022,28 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   if (!s.terms.empty())
     CUDA_TRY(cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  if (s.dense_ok) {
+    // A[p][q][k] += Q, A[p][q][16 + k] += Q or -Q (terms that read conj of pair field q)
+    constexpr int K = kDenseMaxModes;
+    std::vector<double> A((size_t)M * P * 2 * K, 0.0);
+    for (uint32_t p = 0; p < M; ++p)
+      for (int j = s.term_off[p]; j < s.term_off[p + 1]; ++j) {
+        const Term& t = s.terms[j];
+        const size_t q = t.pc & 0x7fff;
+        const double v = t.q;
+        A[((size_t)p * P + q) * 2 * K + t.k] += v;
+        A[((size_t)p * P + q) * 2 * K + K + t.k] += (t.pc & 0x8000) ? -v : v;
+      }
+    const size_t n = A.size();
+    if (b->fp64) {
+      CUDA_TRY(cudaMemcpyAsync((void*)d.dense_q, A.data(), n * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+      CUDA_TRY(cudaStreamSynchronize(b->stream));  // A is a host temporary
+    } else {
+      std::vector<float> Af(A.begin(), A.end());
+      CUDA_TRY(cudaMemcpyAsync((void*)d.dense_q, Af.data(), n * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+      CUDA_TRY(cudaStreamSynchronize(b->stream));  // Af is a host temporary
+    }
+  }
   if (b->raman) {
     // Raman spectrum: H = FFT(h_R) * dt * T0 * fR / NT  (src/MultimodePropagation_CPU.cpp:170-176, :241-251)
     std::vector<double2> hr(nt);
@@ -1040,10 +1083,13 @@ bool batch_shape(mmp_batch* b) {
   uint32_t span = 0;
   size_t max_terms = 0;
   bool iir = b->raman;
+  bool all_dense = true, any_dense = false;
   for (size_t i = 0; i < b->members.size(); ++i) {
     if (!b->active[i]) continue;
     const Member& s = b->members[i];
     iir = iir && s.desc.iir;
+    all_dense = all_dense && s.dense_ok;
+    any_dense = any_dense || s.dense_ok;
     span = (uint32_t)i + 1;
     Mmax = std::max(Mmax, (int)s.M);
     Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
@@ -1068,14 +1114,16 @@ bool batch_shape(mmp_batch* b) {
   if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
     if (std::atoi(env) == 0) fused = false;
   if (fused) smem += scratch;
+  const int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
-  // are read through L1 from the FP64 table)
+  // are read through L1 from the FP64 table); the dense form reads no terms
   const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);
-  const int stage_terms = smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
+  const int stage_terms = dense != 1 && smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
   if (stage_terms) smem += max_terms * staged;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
                        stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
-                       fused != b->raman_fused;
+                       fused != b->raman_fused || dense != b->dense;
+  b->dense = dense;
   b->raman_iir = iir;
   b->raman_fused = fused;
   b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
@@ -1154,6 +1202,7 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->cluster_ctas = (uint32_t)b->ks.C;
   info->raman_recurrence = b->raman_fused ? 2u : (b->raman_iir ? 1u : 0u);
   info->graph_branches = b->groups;
+  info->dense_contraction = (b->dense == 1 || (b->dense == 2 && s.dense_ok)) ? 1u : 0u;
 }
 
 }  // namespace

@@ -1003,9 +1003,32 @@ template <typename T> struct StagedTerm {
   T q;
 };
 
+// 16 consecutive values of T from a 16-byte aligned address, by 16-byte loads
+__device__ __forceinline__ void ld16(const float* a, float* v) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float4 x = __ldg(reinterpret_cast<const float4*>(a) + j);
+    v[4 * j] = x.x; v[4 * j + 1] = x.y; v[4 * j + 2] = x.z; v[4 * j + 3] = x.w;
+  }
+}
+__device__ __forceinline__ void ld16(const double* a, double* v) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const double2 x = __ldg(reinterpret_cast<const double2*>(a) + j);
+    v[2 * j] = x.x; v[2 * j + 1] = x.y;
+  }
+}
+
 // raman_mode: 0 Raman off; 1 the convolutions R arrive as rows (k_pair / k_raman_scan);
 // 2 the recurrence runs through the tile here from the carries of k_raman_carry.
-template <typename T>
+// DENSE = 1: the contraction in its dense form (SolveDesc::dense_q, M <= 16, TT >= 64);
+// DENSE = 2: per solve, the dense form where dense_q is set and the term loop elsewhere
+// (a batch that mixes both; each solve runs the same arithmetic as on its own):
+//   T_pk(t) = sum_q A_re[p][q][k] Re W_q(t) + i sum_q A_im[p][q][k] Im W_q(t),
+//   sigma_p(t) = sum_k U_k(t) T_pk(t),
+// one warp per (p, 64 samples), each lane two samples with all k in registers: a
+// register-blocked matrix product instead of one complex triple product per term.
+template <typename T, int DENSE>
 __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
                                                   int stage_terms, int raman_mode) {
   using V = c2<T>;
@@ -1124,6 +1147,48 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   __syncthreads();
   // 2. contraction
   V* sigma = as_t2<T>(d.sigma);
+  if (DENSE == 1 || (DENSE == 2 && d.dense_q != nullptr)) {
+    constexpr int K = kDenseMaxModes;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const T* A = static_cast<const T*>(d.dense_q);
+    const int chunks = TT >> 6;
+    for (int item = warp; item < M * chunks; item += nwarps) {
+      const int p = item / chunks, tt = ((item - p * chunks) << 6) + 2 * lane;
+      T re0[K], re1[K], im0[K], im1[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) re0[k] = re1[k] = im0[k] = im1[k] = 0;
+      const T* Ap = A + (size_t)p * P * (2 * K);
+#pragma unroll 2
+      for (int q = 0; q < P; ++q) {
+        V w0, w1;
+        ld2<T>(sW + q * TT + tt, w0, w1);
+        T ar[K], ai[K];
+        ld16(Ap + (size_t)q * (2 * K), ar);
+        ld16(Ap + (size_t)q * (2 * K) + K, ai);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          re0[k] = fma(ar[k], w0.x, re0[k]);
+          re1[k] = fma(ar[k], w1.x, re1[k]);
+          im0[k] = fma(ai[k], w0.y, im0[k]);
+          im1[k] = fma(ai[k], w1.y, im1[k]);
+        }
+      }
+      T sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (k < M) {
+          V u0, u1;
+          ld2<T>(sU + k * TT + tt, u0, u1);
+          sx0 = fma(u0.x, re0[k], fma(-u0.y, im0[k], sx0));
+          sy0 = fma(u0.x, im0[k], fma(u0.y, re0[k], sy0));
+          sx1 = fma(u1.x, re1[k], fma(-u1.y, im1[k], sx1));
+          sy1 = fma(u1.x, im1[k], fma(u1.y, re1[k], sy1));
+        }
+      }
+      st2<T>(sigma + (size_t)p * nt + t0 + tt, mk<T>(sx0, sy0), mk<T>(sx1, sy1));
+    }
+    return;
+  }
   for (int idx = threadIdx.x; idx < M * H; idx += blockDim.x) {
     const int p = idx / H, tt = 2 * (idx - p * H);
     T ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;

@@ -198,3 +198,28 @@ def test_raman_recurrence_matches_fft_convolution(mmp, monkeypatch, fp64, nt, wi
     assert mo.rel_l2_per_mode(out_s, out_f).max() < tol
     ref = mo.solve(prob)
     assert mo.rel_l2_per_mode(out_r, ref).max() < (TOL64 if fp64 else TOL32)
+
+
+@pytest.mark.parametrize("fp64", [True, False])
+@pytest.mark.parametrize("raman", [True, False])
+def test_dense_contraction_matches_term_loop_and_oracle(mmp, monkeypatch, fp64, raman):
+    # fully symmetric dense Q (the dense 15-mode workload's construction at M = 5)
+    prob = W.dense15(seed=92, M=5, nt=512, n_steps=8, raman=raman)
+    prob = W.scale_power(prob, W.phase_cap_scale(prob, per_step=0.05, total=0.4))
+    fl = capi.MMP_F_FP64 if fp64 else 0
+    out_d, info_d = run(mmp, prob, [8], fl)
+    monkeypatch.setenv("MMP_DENSE", "0")
+    out_s, info_s = run(mmp, prob, [8], fl)
+    assert (info_d["dense_contraction"], info_s["dense_contraction"]) == (1, 0)
+    assert mo.rel_l2_per_mode(out_d, out_s).max() < (1e-12 if fp64 else 2e-6)
+    assert mo.rel_l2_per_mode(out_d, mo.solve(prob)).max() < (TOL64 if fp64 else TOL32)
+
+
+def test_dense_contraction_forced_on_a_sparse_quirky_case(mmp, monkeypatch):
+    # GRIN-pattern coupling with the reference's pair-slot mapping active: the dense form
+    # built from the resolved terms must reproduce it
+    prob = W.small_case(seed=93, M=4, nt=256, n_steps=6, nnz_target=20).replace(flags=capi.MMP_F_FP64)
+    monkeypatch.setenv("MMP_DENSE", "1")
+    out, info = run(mmp, prob, [6])
+    assert info["dense_contraction"] == 1 and info["pair_quirk_active"] == 1
+    assert mo.rel_l2_per_mode(out, mo.solve(prob)).max() < TOL64
