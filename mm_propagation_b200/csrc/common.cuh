@@ -130,8 +130,10 @@ struct SolveDesc {
   const void* dense_q;
 };
 
-// Largest mode count of the dense contraction form (its accumulators live in registers).
+// Largest mode count of the dense contraction form (its accumulators live in registers),
+// and the coefficient rows a warp stages in shared memory per chunk.
 constexpr int kDenseMaxModes = 16;
+constexpr int kDenseChunk = 16;
 
 // RK tableau passed by value to the stage kernels (identical for a batch).
 struct Tableau {

@@ -1115,6 +1115,7 @@ bool batch_shape(mmp_batch* b) {
     if (std::atoi(env) == 0) fused = false;
   if (fused) smem += scratch;
   const int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
+  if (dense) smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
   // are read through L1 from the FP64 table); the dense form reads no terms
   const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);

@@ -1003,18 +1003,30 @@ template <typename T> struct StagedTerm {
   T q;
 };
 
-// 16 consecutive values of T from a 16-byte aligned address, by 16-byte loads
-__device__ __forceinline__ void ld16(const float* a, float* v) {
+// Ampere-style asynchronous 16-byte copies global -> shared (both 16-byte aligned),
+// grouped and waited for per thread.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// 16 consecutive values of T from 16-byte aligned shared memory, by 16-byte loads
+template <typename T> __device__ __forceinline__ void lds16(const T* a, T* v);
+template <> __device__ __forceinline__ void lds16<float>(const float* a, float* v) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const float4 x = __ldg(reinterpret_cast<const float4*>(a) + j);
+    const float4 x = reinterpret_cast<const float4*>(a)[j];
     v[4 * j] = x.x; v[4 * j + 1] = x.y; v[4 * j + 2] = x.z; v[4 * j + 3] = x.w;
   }
 }
-__device__ __forceinline__ void ld16(const double* a, double* v) {
+template <> __device__ __forceinline__ void lds16<double>(const double* a, double* v) {
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const double2 x = __ldg(reinterpret_cast<const double2*>(a) + j);
+    const double2 x = reinterpret_cast<const double2*>(a)[j];
     v[2 * j] = x.x; v[2 * j + 1] = x.y;
   }
 }
@@ -1047,7 +1059,10 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
   const size_t scratch = raman == 2 ? (size_t)(blockDim.x >> 5) * padded_len(TT) : 0;
-  ST* st = reinterpret_cast<ST*>(sU + (size_t)(M + P) * TT + scratch);
+  // dense form: per warp, two chunks of kDenseChunk coefficient rows (cp.async double buffer)
+  T* sA = reinterpret_cast<T*>(sU + (size_t)(M + P) * TT + scratch);
+  const size_t dense_elems = DENSE ? (size_t)(blockDim.x >> 5) * 2 * kDenseChunk * 2 * kDenseMaxModes : 0;
+  ST* st = reinterpret_cast<ST*>(sA + dense_elems);
   if (stage_terms) {
     for (int j = threadIdx.x; j < n_terms; j += blockDim.x) {
       const Term tm = d.terms[j];
@@ -1150,28 +1165,56 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   if (DENSE == 1 || (DENSE == 2 && d.dense_q != nullptr)) {
     constexpr int K = kDenseMaxModes;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    constexpr int ROW = 2 * K;                       // values per coefficient row (p, q)
+    constexpr int CH = kDenseChunk;                  // rows per staged chunk
+    constexpr int PIECES = CH * ROW * (int)sizeof(T) / 16;  // 16-byte copies per chunk
     const T* A = static_cast<const T*>(d.dense_q);
+    T* sAw = sA + (size_t)warp * 2 * CH * ROW;       // this warp's two chunk buffers
     const int chunks = TT >> 6;
+    const int nchunk = (P + CH - 1) / CH;
     for (int item = warp; item < M * chunks; item += nwarps) {
       const int p = item / chunks, tt = ((item - p * chunks) << 6) + 2 * lane;
       T re0[K], re1[K], im0[K], im1[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) re0[k] = re1[k] = im0[k] = im1[k] = 0;
-      const T* Ap = A + (size_t)p * P * (2 * K);
-#pragma unroll 2
-      for (int q = 0; q < P; ++q) {
-        V w0, w1;
-        ld2<T>(sW + q * TT + tt, w0, w1);
-        T ar[K], ai[K];
-        ld16(Ap + (size_t)q * (2 * K), ar);
-        ld16(Ap + (size_t)q * (2 * K) + K, ai);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          re0[k] = fma(ar[k], w0.x, re0[k]);
-          re1[k] = fma(ar[k], w1.x, re1[k]);
-          im0[k] = fma(ai[k], w0.y, im0[k]);
-          im1[k] = fma(ai[k], w1.y, im1[k]);
+      const T* Ap = A + (size_t)p * P * ROW;
+      // rows q0 .. q0 + CH - 1 (clamped to P) into buffer buf, as one cp.async group
+      auto stage_rows = [&](int buf, int q0) {
+        const int rows = min(CH, P - q0);
+        const int pieces = rows * ROW * (int)sizeof(T) / 16;
+        const char* src = reinterpret_cast<const char*>(Ap + (size_t)q0 * ROW);
+        char* dst = reinterpret_cast<char*>(sAw + (size_t)buf * CH * ROW);
+        for (int i = lane; i < pieces && i < PIECES; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+        cp_async_commit();
+      };
+      __syncwarp();  // the previous item's reads of both buffers are done
+      stage_rows(0, 0);
+      for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) {
+          stage_rows((c + 1) & 1, (c + 1) * CH);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
         }
+        __syncwarp();  // every lane's copies of chunk c have landed
+        const T* rowp = sAw + (size_t)(c & 1) * CH * ROW;
+        const int q0 = c * CH, rows = min(CH, P - q0);
+#pragma unroll 2
+        for (int r = 0; r < rows; ++r) {
+          V w0, w1;
+          ld2<T>(sW + (q0 + r) * TT + tt, w0, w1);
+          T ar[K], ai[K];  // the same addresses on every lane: broadcasts, 16 bytes per load
+          lds16<T>(rowp + r * ROW, ar);
+          lds16<T>(rowp + r * ROW + K, ai);
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            re0[k] = fma(ar[k], w0.x, re0[k]);
+            re1[k] = fma(ar[k], w1.x, re1[k]);
+            im0[k] = fma(ai[k], w0.y, im0[k]);
+            im1[k] = fma(ai[k], w1.y, im1[k]);
+          }
+        }
+        __syncwarp();  // reads of buffer c & 1 done before chunk c + 2 is staged into it
       }
       T sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
 #pragma unroll
