@@ -549,6 +549,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   bool finite = true;
   const int nq = s_nq;
   const double cself = (last ? kp.tab.b[i] : kp.tab.a[i + 1][i]) * h;
+  // spectrum entering the inverse transform: conjugated when it runs as a forward one
+  auto spec_in = [](V v) { return Gm::C == 1 ? cconj(v) : v; };
   constexpr int MAXQ = 6;
   // Fast path, one body per count of stored terms (no predicated dead work): all loads
   // of a chunk of frequencies are issued before its math. Intermediate stages combine
@@ -615,7 +617,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
             xt.y = fma(cq, nj[c][q].y, xt.y);
           }
         }
-        s[pad(li)] = cmul(xt, expi<T>(L * znext));
+        s[pad(li)] = spec_in(cmul(xt, expi<T>(L * znext)));
       }
     }
   };
@@ -666,7 +668,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         }
       }
     }
-    s[pad(li)] = cmul(from_d2<T>(x), expi<T>(L * znext));
+    s[pad(li)] = spec_in(cmul(from_d2<T>(x), expi<T>(L * znext)));
   }
   }
   if (last) {
@@ -701,11 +703,20 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
       }
     }
   }
-  inverse<T, LOGN, XC>(s, sq, kp.tw);
   V* U = as_t2<T>(d.U);
   const T inv = (T)d.inv_nt;
+  if constexpr (Gm::C == 1) {
+    // inverse transform as conj(FFT(conj(x))): the spectrum was stored conjugated, so
+    // this kernel carries the forward transform's code only (a smaller kernel runs its
+    // transforms faster)
+    forward<T, LOGN, XC>(s, sq, kp.tw);
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[(size_t)p * Gm::N + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[(size_t)p * Gm::N + u] = cscale(cconj(s[pad(u)]), inv);
+  } else {
+    inverse<T, LOGN, XC>(s, sq, kp.tw);
+#pragma unroll 8
+    for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[(size_t)p * Gm::N + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
+  }
 }
 
 // ---- k_result: phi_p = IFFT(exp(L_p z) psi_hat_p) / conversion_factor -> io (FP64) --------
