@@ -24,7 +24,9 @@ KernelSet MMP_CAT4(make_kernels_, MMP_TAG, MMP_LOGN, MMP_XC)() {
   KernelSet k;
   k.prime = (const void*)&k_prime<T, L, X>;
   k.pair = (const void*)&k_pair<T, L, X>;
-  k.nu = (const void*)&k_nu<T, L, X>;
+  k.nu = (const void*)&k_nu<T, L, X, -1>;
+  k.nu0 = (const void*)&k_nu<T, L, X, 0>;
+  k.nu3 = (const void*)&k_nu<T, L, X, 3>;
   k.result = (const void*)&k_result<T, L, X>;
   k.dft_fwd = (const void*)&k_dft<T, L, X, false>;
   k.dft_inv = (const void*)&k_dft<T, L, X, true>;

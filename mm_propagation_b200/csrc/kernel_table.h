@@ -7,7 +7,9 @@ namespace mmp {
 struct KernelSet {
   const void* prime = nullptr;
   const void* pair = nullptr;
-  const void* nu = nullptr;
+  const void* nu = nullptr;   // k_nu for any stage
+  const void* nu0 = nullptr;  // ... for stages with 0 stored N_hat_j terms
+  const void* nu3 = nullptr;  // ... for stages with 3
   const void* result = nullptr;
   const void* dft_fwd = nullptr;
   const void* dft_inv = nullptr;

@@ -151,7 +151,7 @@ int ensure_device(int dev, DeviceRes** out) {
       for (int xc = 0; xc < 2; ++xc) {
         KernelSet ks = kernels_for(fp64, L, xc);
         if (!ks.prime) continue;
-        const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.result, ks.dft_fwd, ks.dft_inv};
+        const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.nu0, ks.nu3, ks.result, ks.dft_fwd, ks.dft_inv};
         for (const void* f : fns)
           CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
       }
@@ -577,6 +577,18 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   return MMP_OK;
 }
 
+// The k_nu instantiation for stage i: its count of stored N_hat_j terms (the same count
+// k_nu's thread 0 derives) picks the specialised body, else the generic one.
+const void* nu_kernel(const KernelSet& ks, const Tableau& tab, int i) {
+  int nq = 0;
+  if (i == tab.s - 1) {
+    for (int j = 0; j < tab.s; ++j) nq += (j != i && tab.b[j] != 0.0);
+  } else {
+    for (int j = 0; j < i; ++j) nq += (tab.a[i + 1][j] != 0.0);
+  }
+  return nq == 0 ? ks.nu0 : (nq == 3 ? ks.nu3 : ks.nu);
+}
+
 // Raman pair fields for `nsolves` solves from descs: with the recurrence fused into the
 // contraction, its tile aggregates and carries; else the recurrence as a row scan when
 // every solve's h_R is a damped sinusoid; else the FFT convolution of kernel set ks.
@@ -625,7 +637,7 @@ int time_variant(mmp_batch* b, const KernelSet& ks, float* ms) {
   for (int rep = 0; rep < 4 && rc == MMP_OK; ++rep) {  // rep 0 warms up
     if (rep == 1) cudaEventRecord(e0, b->stream);
     rc = launch_pairs(b, ks, nsol, 0, b->d_descs);
-    if (rc == MMP_OK) rc = launch_row_kernel(b, ks, ks.nu, b->Mmax, nsol, 0, b->d_descs);
+    if (rc == MMP_OK) rc = launch_row_kernel(b, ks, nu_kernel(ks, b->tab, 0), b->Mmax, nsol, 0, b->d_descs);
   }
   cudaEventRecord(e1, b->stream);
   cudaError_t e = cudaEventSynchronize(e1);
@@ -678,7 +690,7 @@ int enqueue_step(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cudaStr
     if (rc) return rc;
     rc = launch_contract(b, first, count, st);
     if (rc) return rc;
-    rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, (int)count, i, descs, st);
+    rc = launch_row_kernel(b, b->ks, nu_kernel(b->ks, b->tab, i), b->Mmax, (int)count, i, descs, st);
     if (rc) return rc;
   }
   return MMP_OK;
@@ -1305,7 +1317,7 @@ int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t
         if (e != cudaSuccess) { rc = fail(MMP_ECUDA, cudaGetErrorString(e)); break; }
         if (kind == 0) rc = launch_pairs(b, b->ks, nsol, i, b->d_descs);
         else if (kind == 1) rc = launch_contract(b);
-        else rc = launch_row_kernel(b, b->ks, b->ks.nu, b->Mmax, nsol, i, b->d_descs);
+        else rc = launch_row_kernel(b, b->ks, nu_kernel(b->ks, b->tab, i), b->Mmax, nsol, i, b->d_descs);
         if (rc) break;
         e = cudaEventRecord(ev[1], b->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);

@@ -460,7 +460,10 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
 }
 
 // ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
-template <typename T, int LOGN, int XC>
+// BODY: the stage arithmetic for exactly BODY stored N_hat_j terms (0 or 3), or -1 for
+// any count. The host launches the instantiation that matches each stage of its tableau
+// (RK4: 0 at the intermediate stages, 3 at the last), so each kernel carries one body.
+template <typename T, int LOGN, int XC, int BODY>
 __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_nu(const KParams kp) {
   using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
@@ -621,13 +624,12 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
       }
     }
   };
-  // Only the counts RK4 needs (0 at intermediate stages, 3 at the last) get their own
-  // body: every extra copy of this loop grows the kernel, and a larger kernel pushes the
-  // transform code out of the instruction cache between calls (measured: the forward
-  // transform ran ~50% slower with seven copies). Other tableaus take the generic loop.
-  if (nq == 0) {
+  // One body per kernel: every extra copy of this loop grows the kernel, and a larger
+  // kernel runs its transforms slower (measured: the forward transform ran ~50% slower
+  // with seven copies). Counts other than 0 and 3 take the generic loop.
+  if constexpr (BODY == 0) {
     body(std::integral_constant<int, 0>{});
-  } else if (nq == 3) {
+  } else if constexpr (BODY == 3) {
     body(std::integral_constant<int, 3>{});
   } else {
 #pragma unroll 2
