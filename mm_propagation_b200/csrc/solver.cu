@@ -577,16 +577,20 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   return MMP_OK;
 }
 
-// The k_nu instantiation for stage i: its count of stored N_hat_j terms (the same count
-// k_nu's thread 0 derives) picks the specialised body, else the generic one.
+// The k_nu instantiation for stage i: an intermediate stage with no stored N_hat_j
+// terms, or a last stage with 3 (the counts k_nu's thread 0 derives), takes its
+// specialised body; every other stage the generic one.
 const void* nu_kernel(const KernelSet& ks, const Tableau& tab, int i) {
+  const bool last = i == tab.s - 1;
   int nq = 0;
-  if (i == tab.s - 1) {
+  if (last) {
     for (int j = 0; j < tab.s; ++j) nq += (j != i && tab.b[j] != 0.0);
   } else {
     for (int j = 0; j < i; ++j) nq += (tab.a[i + 1][j] != 0.0);
   }
-  return nq == 0 ? ks.nu0 : (nq == 3 ? ks.nu3 : ks.nu);
+  if (nq == 0 && !last) return ks.nu0;
+  if (nq == 3 && last) return ks.nu3;
+  return ks.nu;
 }
 
 // Raman pair fields for `nsolves` solves from descs: with the recurrence fused into the

@@ -460,9 +460,10 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
 }
 
 // ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
-// BODY: the stage arithmetic for exactly BODY stored N_hat_j terms (0 or 3), or -1 for
-// any count. The host launches the instantiation that matches each stage of its tableau
-// (RK4: 0 at the intermediate stages, 3 at the last), so each kernel carries one body.
+// BODY: the stage arithmetic of an intermediate stage with no stored N_hat_j terms (0),
+// of a last stage with 3 (3), or of any stage (-1). The host launches the instantiation
+// that matches each stage of its tableau (RK4: 0 at the intermediate stages, 3 at the
+// last), so each kernel carries one body.
 template <typename T, int LOGN, int XC, int BODY>
 __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_nu(const KParams kp) {
   using Gm = Geo<T, LOGN, XC>;
@@ -542,7 +543,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers also publish the values thread 0 wrote
   const int i = kp.stage;
   const int S = kp.tab.s;
-  const bool last = (i == S - 1);
+  // BODY 0 serves intermediate stages only and BODY 3 last stages only: fixed at compile
+  // time, so each instantiation carries only its half of the stage arithmetic
+  const bool last = BODY < 0 ? (i == S - 1) : (BODY == 3);
   const double h = d.dz;
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
