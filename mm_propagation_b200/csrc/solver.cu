@@ -606,7 +606,7 @@ int launch_pairs(mmp_batch* b, const KernelSet& ks, int nsolves, int stage, cons
     int TT = b->TT;
     const SolveDesc* dd = descs;
     void* args[] = {(void*)&dd, &nt, &TT};
-    const int smem = (int)(((size_t)b->Mmax * TT + 8 * (size_t)padded_len(TT)) * t2);
+    const int smem = (int)(((size_t)b->Mmax * TT + TT) * t2);  // U tile and the weight table
     const void* fa = b->fp64 ? (const void*)&k_raman_agg<double> : (const void*)&k_raman_agg<float>;
     CUDA_TRY(launch(fa, dim3((unsigned)(nt / TT), (unsigned)nsolves, 1), 256, smem, 1, st ? st : b->stream, args));
     const void* fc = b->fp64 ? (const void*)&k_raman_carry<double> : (const void*)&k_raman_carry<float>;

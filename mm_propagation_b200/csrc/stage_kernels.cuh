@@ -938,25 +938,44 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
   const int tile = blockIdx.x, t0 = tile * TT;
   if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // The aggregate over the tile from a zero start is a weighted sum,
+  //   S_end = sum_t lambda^(TT-1-t) x_t   (x = Re or Im of U_l conj(U_m)),
+  // so it needs no sequential pass: the weights sit in a table, each lane sums its
+  // samples (32 apart, coalesced) and the warp adds the lanes.
   V* sU = reinterpret_cast<V*>(smem_raw);
-  V* scr = sU + (size_t)d.M * TT + (size_t)warp * padded_len(TT);
+  V* wt = sU + (size_t)d.M * TT;
   stage_u_tile<T>(sU, d, nt, t0, TT);
+  for (int t = threadIdx.x; t < TT; t += blockDim.x) {  // lambda^(TT-1-t), FP64 powers
+    double2 r = make_double2(1.0, 0.0), b = d.iir_lambda;
+    for (int e = TT - 1 - t; e; e >>= 1) {
+      if (e & 1) r = cmul(r, b);
+      b = cmul(b, b);
+    }
+    wt[t] = from_d2<T>(r);
+  }
   __syncthreads();
-  TileScan<T> ts;
-  ts.init(d, TT >> 5, lane);
   const int ntiles = nt / TT;
   V* out = as_t2<T>(d.raman_tiles);
   for (int q = warp; q < d.P; q += nwarps) {
-    ts.form(sU, TT, d.pairs[q], scr, lane);
-    __syncwarp();
-    V la, lb;
-    ts.lane_local(scr, lane, la, lb);
-    ts.lane_scan(la, lb, lane);
-    if (lane == 31) {  // the whole tile
-      out[((size_t)q * ntiles + tile) * 2] = la;
-      out[((size_t)q * ntiles + tile) * 2 + 1] = lb;
+    const int2 lm = d.pairs[q];
+    V sa = mk<T>(0, 0), sb = mk<T>(0, 0);
+    for (int t = lane; t < TT; t += 32) {
+      const V x = cmulc(sU[lm.x * TT + t], sU[lm.y * TT + t]);
+      const V w = wt[t];
+      sa = mk<T>(fma(w.x, x.x, sa.x), fma(w.y, x.x, sa.y));
+      sb = mk<T>(fma(w.x, x.y, sb.x), fma(w.y, x.y, sb.y));
     }
-    __syncwarp();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sa.x += __shfl_xor_sync(0xffffffffu, sa.x, o);
+      sa.y += __shfl_xor_sync(0xffffffffu, sa.y, o);
+      sb.x += __shfl_xor_sync(0xffffffffu, sb.x, o);
+      sb.y += __shfl_xor_sync(0xffffffffu, sb.y, o);
+    }
+    if (lane == 0) {
+      out[((size_t)q * ntiles + tile) * 2] = sa;
+      out[((size_t)q * ntiles + tile) * 2 + 1] = sb;
+    }
   }
 }
 
