@@ -81,31 +81,41 @@ def parse():
 
 # ---- process-group plumbing ----------------------------------------------------------------
 class Dist:
+    """One process per GPU (torchrun env). The ranks are replicas: each runs its own batch
+    of independent solves; the only collectives are a barrier and the max of the timings.
+    Backend NCCL on GPUs; MMP_DIST_BACKEND=gloo runs the same plumbing on CPU (tests)."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = os.environ.get("MMP_DIST_BACKEND", "nccl")
         self.pg = None
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(self.local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+            td.init_process_group(self.backend, timeout=datetime.timedelta(seconds=300))
             self.pg = td
+
+    def _device(self):
+        return "cuda" if self.backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
             import torch
-            t = torch.zeros(1, device="cuda")
+            t = torch.zeros(1, device=self._device())
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                torch.cuda.synchronize()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self._device())
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
