@@ -1123,13 +1123,10 @@ bool batch_shape(mmp_batch* b) {
   if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
     if (std::atoi(env) == 1) iir = false;
   // the recurrence runs inside the contraction tiles when a lane gets 2..8 samples
-  // (64 <= TT <= 256) and the per-warp scratch rows fit; MMP_RAMAN_FUSED=0 keeps the row scan
+  // (64 <= TT <= 256); MMP_RAMAN_FUSED=0 keeps the row scan
   bool fused = iir && TT >= 64 && (int)b->nt >= TT;
-  const size_t scratch = 8 * (size_t)padded_len(TT) * t2;
-  if (fused && smem + scratch > 200 * 1024) fused = false;
   if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
     if (std::atoi(env) == 0) fused = false;
-  if (fused) smem += scratch;
   const int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
   if (dense) smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they

@@ -846,13 +846,13 @@ constexpr unsigned kMaxWaitPolls = 1u << 24;  // far above any copy time; then r
 //   k_contract     (mode 2) runs the recurrence through its own tile from that state
 //                  and forms W = (1 - f_R) V + R in shared memory; R never leaves the SM.
 // Within a tile one warp handles one pair field at a time, lane L owning samples
-// [c L, c L + c); V is staged in a per-warp padded scratch row so that both the
-// coalesced fill (sample 32 j + L) and the lane-contiguous scan read without conflicts
-// beyond 2-way.
+// [c L, c L + c). The pair field row is written once, coalesced, in a swizzled layout
+// (wsw) in which a lane's c samples are also conflict-free 16-byte loads; the lane keeps
+// them in registers through the scan and writes W back in place, in the same layout.
 template <typename T> struct TileScan {
   using V = c2<T>;
   V lt, kt;
-  V pw[8];      // lambda^(k+1)
+  V rw[8];      // lambda^(c-1-k): weights of the lane's local aggregate
   V lvl[5];     // lambda^(c 2^j): the multipliers of the lane scan's levels
   V lane_pow;   // lambda^(c lane): carries the tile's entering state to this lane
   int c;
@@ -861,19 +861,19 @@ template <typename T> struct TileScan {
     const double2 lam = d.iir_lambda;
     lt = from_d2<T>(lam);
     kt = from_d2<T>(d.iir_kappa);
-    double2 p = lam, lamc = lam;
+    double2 p = make_double2(1.0, 0.0);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      pw[k] = from_d2<T>(p);
-      if (k + 1 == c) lamc = p;
-      p = cmul(p, lam);
+    for (int k = 7; k >= 0; --k) {
+      rw[k] = from_d2<T>(p);
+      if (k < c) p = cmul(p, lam);
     }
+    // p = lambda^c
     double2 lp = make_double2(1.0, 0.0);
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
-      lvl[j] = from_d2<T>(lamc);
-      if ((lane >> j) & 1) lp = cmul(lp, lamc);
-      lamc = cmul(lamc, lamc);
+      lvl[j] = from_d2<T>(p);
+      if ((lane >> j) & 1) lp = cmul(lp, p);
+      p = cmul(p, p);
     }
     lane_pow = from_d2<T>(lp);
   }
@@ -896,27 +896,13 @@ template <typename T> struct TileScan {
   __device__ __forceinline__ V step(V s, T x) const {
     return mk<T>(fma(lt.x, s.x, fma(-lt.y, s.y, x)), fma(lt.x, s.y, lt.y * s.x));
   }
-  // V = U_l conj(U_m) of the tile into the scratch row
-  __device__ __forceinline__ void form(const V* sU, int TT, int2 lm, V* scr, int lane) const {
-    for (int j = 0; j < c; ++j) {
-      const int e = 32 * j + lane;
-      scr[pad(e)] = cmulc(sU[lm.x * TT + e], sU[lm.y * TT + e]);
-    }
-  }
-  // this lane's recurrence over its samples from a zero start
-  __device__ __forceinline__ void lane_local(const V* scr, int lane, V& la, V& lb) const {
-    la = mk<T>(0, 0);
-    lb = mk<T>(0, 0);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (k < c) {
-        const V x = scr[pad(c * lane + k)];
-        la = step(la, x.x);
-        lb = step(lb, x.y);
-      }
-    }
-  }
 };
+
+// Position of the sample pair (2h, 2h + 1) in a pair-field row of the contraction tile:
+// 16-byte chunk h ^ ((h >> 3) & mask). With mask = TT/64 - 1 (TT = 128, 256) both a
+// warp's 32 consecutive chunks and lane L's chunks [g L, g L + g) (g = TT/64) fall on
+// distinct banks per quarter warp; mask 0 is the plain layout.
+__device__ __forceinline__ int wsw(int h, int mask) { return h ^ ((h >> 3) & mask); }
 
 template <typename T>
 __device__ __forceinline__ void stage_u_tile(c2<T>* sU, const SolveDesc& d, int nt, int t0, int TT) {
@@ -1076,7 +1062,7 @@ template <> __device__ __forceinline__ void lds16<double>(const double* a, doubl
 // one warp per (p, 64 samples), each lane two samples with all k in registers: a
 // register-blocked matrix product instead of one complex triple product per term.
 template <typename T, int DENSE>
-__global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
+__global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
                                                   int stage_terms, int raman_mode) {
   using V = c2<T>;
   using ST = StagedTerm<T>;
@@ -1093,9 +1079,10 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   const T kerr = (T)d.one_minus_fR;
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
-  const size_t scratch = raman == 2 ? (size_t)(blockDim.x >> 5) * padded_len(TT) : 0;
+  // pair-field rows: swizzled (wsw) when the recurrence runs here, else plain
+  const int wmask = raman == 2 ? max(TT >> 6, 1) - 1 : 0;
   // dense form: per warp, two chunks of kDenseChunk coefficient rows (cp.async double buffer)
-  T* sA = reinterpret_cast<T*>(sU + (size_t)(M + P) * TT + scratch);
+  T* sA = reinterpret_cast<T*>(sU + (size_t)(M + P) * TT);
   const size_t dense_elems = DENSE ? (size_t)(blockDim.x >> 5) * 2 * kDenseChunk * 2 * kDenseMaxModes : 0;
   ST* st = reinterpret_cast<ST*>(sA + dense_elems);
   if (stage_terms) {
@@ -1147,18 +1134,37 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
       }
       st2<T>(sW + q * TT + tt, w0, w1);
     }
-  } else {  // one warp per pair field: the recurrence through the tile, then W
+  } else {  // one warp per pair field: the recurrence through the tile, then W in place
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    V* scr = sW + (size_t)P * TT + (size_t)warp * padded_len(TT);
     TileScan<T> ts;
     ts.init(d, TT >> 5, lane);
+    const int c = ts.c, g = c >> 1;  // samples and sample pairs per lane (TT >= 64)
     const int ntiles = nt / TT;
     const V* tiles = as_t2<T>(d.raman_tiles);
     for (int q = warp; q < P; q += nwarps) {
-      ts.form(sU, TT, d.pairs[q], scr, lane);
+      const int2 lm = d.pairs[q];
+      V* row = sW + (size_t)q * TT;
+      // V = U_l conj(U_m), coalesced over the sample pairs
+      for (int h = lane; h < H; h += 32) {
+        V ul0, ul1, um0, um1;
+        ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
+        ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
+        st2<T>(row + 2 * wsw(h, wmask), cmulc(ul0, um0), cmulc(ul1, um1));
+      }
       __syncwarp();
-      V la, lb;
-      ts.lane_local(scr, lane, la, lb);
+      V x[8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < g) ld2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+      // this lane's aggregate from a zero start: sum_k lambda^(c-1-k) x_k, x_k = Re or Im V
+      V la = mk<T>(0, 0), lb = mk<T>(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k < c) {
+          la = mk<T>(fma(ts.rw[k].x, x[k].x, la.x), fma(ts.rw[k].y, x[k].x, la.y));
+          lb = mk<T>(fma(ts.rw[k].x, x[k].y, lb.x), fma(ts.rw[k].y, x[k].y, lb.y));
+        }
+      }
       ts.lane_scan(la, lb, lane);
       // state entering this lane's samples: lambda^(c lane) C_tile + earlier lanes
       V ea, eb;
@@ -1168,30 +1174,21 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
       eb.y = __shfl_up_sync(0xffffffffu, lb.y, 1);
       if (lane == 0) ea = eb = mk<T>(0, 0);
       const size_t ti = ((size_t)q * ntiles + blockIdx.x) * 2;
-      const V Ca = cadd(cmul(ts.lane_pow, tiles[ti]), ea);
-      const V Cb = cadd(cmul(ts.lane_pow, tiles[ti + 1]), eb);
-      const V kca = cmul(ts.kt, Ca), kcb = cmul(ts.kt, Cb);
-      la = mk<T>(0, 0);
-      lb = mk<T>(0, 0);
+      V sa = cadd(cmul(ts.lane_pow, tiles[ti]), ea);
+      V sb = cadd(cmul(ts.lane_pow, tiles[ti + 1]), eb);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        if (k < ts.c) {
-          V& cell = scr[pad(ts.c * lane + k)];
-          const V x = cell;
-          la = ts.step(la, x.x);
-          lb = ts.step(lb, x.y);
-          // R = Im(kappa local) + Im(lambda^(k+1) kappa C), W = (1 - f_R) V + R
-          const T rx = fma(ts.kt.x, la.y, fma(ts.kt.y, la.x, fma(ts.pw[k].x, kca.y, ts.pw[k].y * kca.x)));
-          const T ry = fma(ts.kt.x, lb.y, fma(ts.kt.y, lb.x, fma(ts.pw[k].x, kcb.y, ts.pw[k].y * kcb.x)));
-          cell = mk<T>(fma(kerr, x.x, rx), fma(kerr, x.y, ry));
+        if (k < c) {
+          sa = ts.step(sa, x[k].x);
+          sb = ts.step(sb, x[k].y);
+          // R = Im(kappa S), W = (1 - f_R) V + R
+          x[k] = mk<T>(fma(kerr, x[k].x, fma(ts.kt.x, sa.y, ts.kt.y * sa.x)),
+                       fma(kerr, x[k].y, fma(ts.kt.x, sb.y, ts.kt.y * sb.x)));
         }
       }
-      __syncwarp();
-      for (int j = 0; j < ts.c; ++j) {
-        const int e = 32 * j + lane;
-        sW[q * TT + e] = scr[pad(e)];
-      }
-      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < g) st2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
     }
   }
   __syncthreads();
@@ -1209,6 +1206,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
     const int nchunk = (P + CH - 1) / CH;
     for (int item = warp; item < M * chunks; item += nwarps) {
       const int p = item / chunks, tt = ((item - p * chunks) << 6) + 2 * lane;
+      const int tw = 2 * wsw(tt >> 1, wmask);
       T re0[K], re1[K], im0[K], im1[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) re0[k] = re1[k] = im0[k] = im1[k] = 0;
@@ -1237,7 +1235,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
 #pragma unroll 2
         for (int r = 0; r < rows; ++r) {
           V w0, w1;
-          ld2<T>(sW + (q0 + r) * TT + tt, w0, w1);
+          ld2<T>(sW + (q0 + r) * TT + tw, w0, w1);
           T ar[K], ai[K];  // the same addresses on every lane: broadcasts, 16 bytes per load
           lds16<T>(rowp + r * ROW, ar);
           lds16<T>(rowp + r * ROW + K, ai);
@@ -1269,6 +1267,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
   }
   for (int idx = threadIdx.x; idx < M * H; idx += blockDim.x) {
     const int p = idx / H, tt = 2 * (idx - p * H);
+    const int tw = 2 * wsw(tt >> 1, wmask);
     T ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
     const int j1 = d.term_off[p + 1];
     for (int j = d.term_off[p]; j < j1; ++j) {
@@ -1283,7 +1282,7 @@ __global__ void __launch_bounds__(256) k_contract(const SolveDesc* __restrict__ 
       }
       V u0, u1, w0, w1;
       ld2<T>(sU + k * TT + tt, u0, u1);
-      ld2<T>(sW + (pc & 0x7fff) * TT + tt, w0, w1);
+      ld2<T>(sW + (pc & 0x7fff) * TT + tw, w0, w1);
       if (pc & 0x8000) {
         w0.y = -w0.y;
         w1.y = -w1.y;
