@@ -43,14 +43,22 @@ __device__ __forceinline__ double im_L(const double* poly, int nb, double alpha)
   return r;
 }
 
+// Small integer -> double without the conversion unit: the bits 0x43300000:(j + 2^31) are
+// the double 2^52 + 2^31 + j (exact for |j| < 2^31), so one subtraction leaves j.
+__device__ __forceinline__ double int_to_double(int j) {
+  return __hiloint2double(0x43300000, (int)((unsigned)j ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 __device__ __forceinline__ double alpha_of(int k, int nt, double alpha_scale) {
   // src/MultimodePropagation.cpp:167-171: index j <= nt/2 -> j, else j - nt
   const int kk = (k <= (nt >> 1)) ? k : k - nt;
-  return alpha_scale * (double)kk;
+  return alpha_scale * int_to_double(kk);
 }
 
 // exp(i theta) with theta reduced in FP64 (Cody–Waite with a two-part constant).
-// FP32: reduced by pi/2 to x in [-pi/4, pi/4] and quadrant n mod 4, then the Taylor
+// FP32: reduced by pi/2 to x in [-pi/4, pi/4] and quadrant n mod 4 (n = theta 2/pi rounded
+// by adding 1.5 * 2^52, whose ulp is 1: n and its low bits come out of one FMA, with
+// no conversion instruction; valid for |theta 2/pi| < 2^51), then the Taylor
 // series of sin and cos to x^9 and x^10 (truncation below 2e-9 on that interval),
 // evaluated by Horner in x^2 in FP32; the quadrant swaps and negates. Short, branch-free
 // code with no large-argument path (the argument is already small). FP64: reduced by
@@ -60,7 +68,9 @@ template <typename T> __device__ __forceinline__ c2<T> expi(double theta) {
     constexpr double k2OverPi = 0.63661977236758134308;
     constexpr double kHalfPiHi = 1.57079632679489655800;    // nearest double to pi/2
     constexpr double kHalfPiLo = 6.12323399573676603587e-17;  // pi/2 - kHalfPiHi
-    const double n = rint(theta * k2OverPi);
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    const double t = fma(theta, k2OverPi, kRound);
+    const double n = t - kRound;
     const double r = fma(-n, kHalfPiLo, fma(-n, kHalfPiHi, theta));
     const float x = (float)r, x2 = x * x;
     // sin x = x (1 - x^2/3! + x^4/5! - x^6/7! + x^8/9!), cos x = 1 - x^2/2! + ... - x^10/10!
@@ -70,7 +80,7 @@ template <typename T> __device__ __forceinline__ c2<T> expi(double theta) {
         x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -1.0f / 3628800.0f, 1.0f / 40320.0f), -1.0f / 720.0f), 1.0f / 24.0f),
                  -0.5f),
         1.0f);
-    const int q = (int)(long long)n & 3;
+    const int q = __double2loint(t) & 3;
     const float c = (q & 1) ? sp : cp, s = (q & 1) ? cp : sp;
     return make_float2((q == 1 || q == 2) ? -c : c, (q >= 2) ? -s : s);
   } else {
@@ -562,6 +572,10 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // of a chunk of frequencies are issued before its math. Intermediate stages combine
   // x_hat in T (it only feeds the nonlinearity, which runs in T); the last stage
   // accumulates psi_{n+1} in FP64.
+  // E_{i+1} = E_i when z does not move between the stages (RK4: c_2 = c_3, c_4 = 1)
+  const bool same_z = zi == znext;
+  float p_part_f = 0.0f;
+  const float w0f = (float)d.omega0_T0, asf = (float)d.alpha_scale;
   auto body = [&](auto nqc) {
     constexpr int NQ = decltype(nqc)::value;
     constexpr int CHK = 2 < Gm::E ? 2 : Gm::E;
@@ -588,13 +602,37 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         const double alpha = alpha_of(k, Gm::N, d.alpha_scale);
         const double L = nb3 ? fma(fma(poly[2], alpha, poly[1]), alpha, poly[0]) : im_L(poly, d.n_beta, alpha);
         // N_hat_i = i sgn(gamma) conj(E_i) FFT(sigma)   (src/MultimodePropagation_CPU.cpp:231-237)
-        const V xe = cmulc(sv[c], expi<T>(L * zi));
+        const V ei = expi<T>(L * zi);
+        const V xe = cmulc(sv[c], ei);
         V nh;
         nh.x = (T)(-d.sgn_gamma) * xe.y;
         nh.y = (T)(d.sgn_gamma) * xe.x;
         Nh[(size_t)i * mstride + row + k] = nh;
         V xt;
-        if (last) {
+        if (last && sizeof(T) == 4) {
+          // psi_{n+1} = psi_n + inc in FP64; the increment h sum_j b_j N_j is formed in
+          // FP32 from the FP32 N_j (its rounding is that of the N_j themselves), so the
+          // only conversions are inc -> FP64 and psi_{n+1} -> FP32
+          V inc = mk<T>((T)cself * nh.x, (T)cself * nh.y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) {
+            const T cq = (T)s_cq[q];
+            inc.x = fma(cq, nj[c][q].x, inc.x);
+            inc.y = fma(cq, nj[c][q].y, inc.y);
+          }
+          const double2 x = make_double2(ps[c].x + (double)inc.x, ps[c].y + (double)inc.y);
+          d.psi_hat[row + k] = x;
+          const double a2 = x.x * x.x + x.y * x.y;
+          finite = finite && isfinite(a2);
+          e_part += a2;
+          xt = from_d2<T>(x);
+          // photon monitor in FP32 (per-thread partial sums; FP64 across threads)
+          if (w0f != 0.0f) {
+            const int kk = (k <= (Gm::N >> 1)) ? k : k - Gm::N;
+            const float af = __int_as_float(0x4B400000 + kk) - 12582912.0f;  // kk as float, exact
+            p_part_f += __fdividef(xt.x * xt.x + xt.y * xt.y, fmaf(asf, af, w0f));
+          }
+        } else if (last) {
           const double2 nhd = to_d2(nh);
           double2 x = ps[c];
           x.x = fma(cself, nhd.x, x.x);
@@ -623,7 +661,10 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
             xt.y = fma(cq, nj[c][q].y, xt.y);
           }
         }
-        s[pad(li)] = spec_in(cmul(xt, expi<T>(L * znext)));
+        V en;
+        if (same_z) en = ei;
+        else en = expi<T>(L * znext);
+        s[pad(li)] = spec_in(cmul(xt, en));
       }
     }
   };
@@ -676,6 +717,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     s[pad(li)] = spec_in(cmul(from_d2<T>(x), expi<T>(L * znext)));
   }
   }
+  p_part += (double)p_part_f;
   if (last) {
     // Block reduction of the monitors, then the last CTA of this solve advances the
     // step. Done before the inverse transform, so none of it is live across that call;

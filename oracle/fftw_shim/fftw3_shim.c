@@ -13,6 +13,7 @@
  * plan) concurrently from OpenMP threads, as it does in
  * src/MultimodePropagation_CPU.cpp:114-119 and :136-163.
  */
+#define _POSIX_C_SOURCE 200112L /* posix_memalign under -std=c11 */
 #include "fftw3.h"
 
 #include <math.h>

@@ -223,3 +223,18 @@ def test_dense_contraction_forced_on_a_sparse_quirky_case(mmp, monkeypatch):
     out, info = run(mmp, prob, [6])
     assert info["dense_contraction"] == 1 and info["pair_quirk_active"] == 1
     assert mo.rel_l2_per_mode(out, mo.solve(prob)).max() < TOL64
+
+
+def test_fp32_monitors_match_fp64(mmp):
+    # energy and photon-number monitors (center frequency of 1550 nm light) of the FP32-bulk
+    # path against the FP64 path: FP64 accumulation in both, FP32 photon weights in the former
+    prob = W.grin2(seed=4, nt=1024, n_steps=1000, peak_scale=0.01).replace(center_frequency=1215.2)
+    mons = []
+    for fl in (0, capi.MMP_F_FP64):
+        with mmp.Solver(prob.replace(flags=fl)) as s:
+            s.propagate(100)
+            mons.append(s.monitors())
+    (e32, p32), (e64, p64) = mons
+    assert len(e32) == len(p32) == 100 and p64.min() > 0
+    assert np.abs(e32 / e64 - 1).max() < 1e-6
+    assert np.abs(p32 / p64 - 1).max() < 1e-5
