@@ -381,7 +381,11 @@ def ours_arm(args, dist):
                     + n_pairs * p.nt * (16 if args.fp64 else 8)) for p in probs) / 1e6
     for _ in range(args.warmup):
         batch.propagate(R)
+    info = batch.info(0)  # after the first propagate: the autotuned kernel choices
+    chosen = {"row_ctas": info["cluster_ctas"], "raman_recurrence": info["raman_recurrence"],
+              "dense_contraction": info["dense_contraction"], "graph_branches": info["graph_branches"]}
     if args.profile_only:
+        print(json.dumps({"kernels_chosen": chosen}))
         batch.propagate(R)
         return None
     # per-kernel device times (un-graphed, one event pair per launch)
@@ -498,7 +502,8 @@ def ours_arm(args, dist):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32", "data": "synthetic",
-        "config": {**workload_config(args, probe, dist.world), "state_mb_per_gpu": round(state_mb, 1)},
+        "config": {**workload_config(args, probe, dist.world), "state_mb_per_gpu": round(state_mb, 1),
+                   "kernels_chosen": chosen},
         "roofline": roof, "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
                 "rk_steps_per_e2e_step": nsteps,
