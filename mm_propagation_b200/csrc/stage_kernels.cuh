@@ -148,6 +148,26 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   }
 }
 
+// Ampere-style asynchronous copies global -> shared (both addresses aligned to the size),
+// grouped and waited for per thread: the loads are in flight without holding registers.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+// one complex value of T
+template <typename T> __device__ __forceinline__ void cp_async_c2(c2<T>* smem_dst, const c2<T>* gmem_src) {
+  if constexpr (sizeof(c2<T>) == 8) cp_async8(smem_dst, gmem_src);
+  else cp_async16(smem_dst, gmem_src);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <typename G> __device__ __forceinline__ int cluster_rank() {
   if constexpr (G::C == 1) return 0;
   else return (int)cg::this_cluster().block_rank();
@@ -482,14 +502,32 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   __shared__ double poly[kMaxBeta];
   __shared__ double red[2][32];
   __shared__ SolveDesc sdesc;
-  stage_desc(&sdesc, kp.descs + blockIdx.y);
-  const V* sq = load_twiddles<T, LOGN, XC>(smem_raw, kp.tw);
-  __syncthreads();
-  const SolveDesc& d = sdesc;
   const int p = blockIdx.x / Gm::C;
-  if (p >= d.M || __ldcg(d.step) >= d.step_limit) return;  // uniform over the cluster
   const int rank = cluster_rank<Gm>();
   const int tid = threadIdx.x;
+  // The sigma row and the twiddle table start on their way first, as asynchronous copies
+  // into shared memory (all of a thread's elements in flight, no registers held): the row's
+  // address and the mode count come straight from the descriptor in global memory, so
+  // the descriptor and polynomial round trips below overlap the row's.
+  V* sq = reinterpret_cast<V*>(smem_raw + Gm::DATA_BYTES);
+  {
+    const c2<T>* g = tw_table<T>(kp.tw, Gm::LOGL);
+    for (int m = tid; m < Gm::NL / 4; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
+    const SolveDesc* gd = kp.descs + blockIdx.y;
+    if (p < __ldg(&gd->M)) {
+      const V* sg = as_t2<T>(reinterpret_cast<const void*>(__ldg(reinterpret_cast<const unsigned long long*>(&gd->sigma)))) +
+                    (size_t)p * Gm::N;
+      for (int u = tid; u < Gm::NL; u += Gm::NTHR) cp_async_c2<T>(&s[pad(u)], sg + Gm::time_of(rank, u));
+    }
+    cp_async_commit();
+  }
+  stage_desc(&sdesc, kp.descs + blockIdx.y);
+  __syncthreads();
+  const SolveDesc& d = sdesc;
+  if (p >= d.M || __ldcg(d.step) >= d.step_limit) {  // uniform over the cluster
+    cp_async_wait<0>();  // no copy may land after the CTA has left
+    return;
+  }
   load_poly(poly, d, p);
   // Scalars needed after the forward transform live in shared memory rather than in
   // registers, so the (out-of-line) transform call has little to save and restore.
@@ -527,20 +565,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     }
     s_nq = nq;
   }
-  const V* sig = as_t2<T>(d.sigma);
-  if constexpr (Gm::C == 1 && sizeof(T) == 4) {
-    const float4* sg = reinterpret_cast<const float4*>(sig + (size_t)p * Gm::N);
-#pragma unroll 8
-    for (int u2 = tid; u2 < Gm::NL / 2; u2 += Gm::NTHR) {
-      const float4 a = sg[u2];
-      s[pad(2 * u2)] = make_float2(a.x, a.y);
-      s[pad(2 * u2 + 1)] = make_float2(a.z, a.w);
-    }
-  } else {
-#pragma unroll 8
-    for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = sig[(size_t)p * Gm::N + Gm::time_of(rank, u)];
-  }
-  if (tid == 0) {  // after this thread's sigma loads, so the prefetches do not delay them
+  if (tid == 0) {
     const size_t prow = (size_t)p * Gm::N;
     const size_t pstride = (size_t)d.M * Gm::N;
     const V* Nq = as_t2<T>(d.Nh);
@@ -550,7 +575,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
       for (int q = 0; q < s_nq; ++q) prefetch_l2(Nq + (size_t)s_jq[q] * pstride + f0, Gm::CH * (unsigned)sizeof(V));
     }
   }
-  forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers also publish the values thread 0 wrote
+  cp_async_wait<0>();                  // this thread's sigma and twiddle copies
+  forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers publish them and the values thread 0 wrote
   const int i = kp.stage;
   const int S = kp.tab.s;
   // BODY 0 serves intermediate stages only and BODY 3 last stages only: fixed at compile
@@ -578,7 +604,10 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   const float w0f = (float)d.omega0_T0, asf = (float)d.alpha_scale;
   auto body = [&](auto nqc) {
     constexpr int NQ = decltype(nqc)::value;
-    constexpr int CHK = 2 < Gm::E ? 2 : Gm::E;
+    // frequencies per chunk: all of a chunk's loads are in flight together (8 when the
+    // stage reads only psi_hat)
+    constexpr int CHK0 = NQ == 0 ? 8 : 2;
+    constexpr int CHK = CHK0 < Gm::E ? CHK0 : Gm::E;
     const double nb3 = d.n_beta == 3;
 #pragma unroll 1
     for (int e0 = 0; e0 < Gm::E; e0 += CHK) {
@@ -1065,17 +1094,6 @@ template <typename T> struct StagedTerm {
   unsigned short k, pc;
   T q;
 };
-
-// Ampere-style asynchronous 16-byte copies global -> shared (both 16-byte aligned),
-// grouped and waited for per thread.
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // 16 consecutive values of T from 16-byte aligned shared memory, by 16-byte loads
 template <typename T> __device__ __forceinline__ void lds16(const T* a, T* v);
