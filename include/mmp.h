@@ -111,6 +111,8 @@ typedef struct mmp_info {
   uint32_t graph_branches;                  /* independent solve groups per captured graph */
   uint32_t dense_contraction;               /* 1: the contraction runs as a dense register-blocked
                                                product over (p, k) x pair fields (M <= 16) */
+  uint32_t tensor_core_contraction;         /* 1: that dense product runs on the tensor cores
+                                               (tcgen05, TF32 operands split hi + lo, FP32 sums) */
 } mmp_info;
 
 typedef struct mmp_solver mmp_solver;

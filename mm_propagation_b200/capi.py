@@ -77,6 +77,7 @@ class mmp_info(C.Structure):
         ("raman_recurrence", C.c_uint32),
         ("graph_branches", C.c_uint32),
         ("dense_contraction", C.c_uint32),
+        ("tensor_core_contraction", C.c_uint32),
     ]
 
 

@@ -128,12 +128,22 @@ struct SolveDesc {
   // entry (p, q, k) sums Q over the terms of p with U_k and pair field q, entry
   // (p, q, kDenseMaxModes + k) the same with the sign of conj-read terms; null if unused
   const void* dense_q;
+  // The same coefficients for the tensor-core form (FP32 solves): per chunk of kTcChunk pair
+  // fields, four K-major matrices [Re hi, Re lo, Im hi, Im lo][kTcChunk/4][16 M][4] of
+  // TF32 values (x = hi + lo), row (p, k) = 16 p + k; null if unused
+  const float* dense_tc;
 };
 
 // Largest mode count of the dense contraction form (its accumulators live in registers),
 // and the coefficient rows a warp stages in shared memory per chunk.
 constexpr int kDenseMaxModes = 16;
 constexpr int kDenseChunk = 16;
+// Tensor-core form of the dense contraction: samples per tile (the MMA's M), pair fields
+// per K chunk, and the fewest modes a solve needs for it (from 6 modes, 21 pair fields,
+// on; below that the register-blocked form costs less than a tile's MMA pipeline).
+constexpr int kTcTile = 128;
+constexpr int kTcChunk = 16;
+constexpr int kTcMinModes = 6;
 
 // RK tableau passed by value to the stage kernels (identical for a batch).
 struct Tableau {

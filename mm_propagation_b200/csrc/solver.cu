@@ -160,6 +160,8 @@ int ensure_device(int dev, DeviceRes** out) {
                                 (const void*)&k_contract<double, 1>, (const void*)&k_contract<double, 2>};
   for (const void* f : contract_fns)
     CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                200 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
@@ -478,6 +480,7 @@ struct mmp_batch {
   bool raman_iir = false;  // every solve's h_R is a damped sinusoid: pair fields by k_raman_scan
   bool raman_fused = false;  // ... and the recurrence runs inside the contraction tiles
   int dense = 0;  // contraction form: 0 term loop, 1 dense (k_contract<T, 1>), 2 per solve
+  bool tc = false;  // dense form on the tensor cores (k_contract_tc)
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -572,6 +575,11 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
                        (const void*)&k_contract<float, 2>};
   const void* f64[] = {(const void*)&k_contract<double, 0>, (const void*)&k_contract<double, 1>,
                        (const void*)&k_contract<double, 2>};
+  if (b->tc) {
+    void* targs[] = {(void*)&descs, &nt, &mode};
+    CUDA_TRY(launch((const void*)&k_contract_tc<float>, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, targs));
+    return MMP_OK;
+  }
   const void* fn = b->fp64 ? f64[b->dense] : f32[b->dense];
   CUDA_TRY(launch(fn, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, args));
   return MMP_OK;
@@ -888,6 +896,40 @@ bool same_shape(const mmp_batch* b, const mmp_params* p) {
          std::memcmp(&t, &b->tab, sizeof(t)) == 0;
 }
 
+// Tensor-core form of the dense coefficients (SolveDesc::dense_tc): floats per solve, and
+// the matrices themselves from the FP64 dense form A[p][q][0..31]. Per chunk of kTcChunk
+// pair fields: four K-major matrices [Re hi, Re lo, Im hi, Im lo][kTcChunk/4][N = 16 M][4],
+// row n = 16 p + k, each value split x = hi + lo with hi = x rounded to TF32 (nearest, ties
+// away, as the device's cvt.rna) and lo = x - hi in FP32; rows k >= M and fields q >= P are 0.
+size_t tc_floats(size_t M, size_t P) {
+  const size_t nch = (P + kTcChunk - 1) / kTcChunk;
+  return nch * 4 * kTcChunk * 16 * M;
+}
+float tf32_round(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u = (u + 0x1000u) & 0xFFFFE000u;
+  std::memcpy(&x, &u, 4);
+  return x;
+}
+std::vector<float> tc_operand(const std::vector<double>& A, int M, int P) {
+  constexpr int K = kDenseMaxModes, KC = kTcChunk;
+  const int N = 16 * M, nch = (P + KC - 1) / KC;
+  std::vector<float> B(tc_floats(M, P), 0.0f);
+  for (int c = 0; c < nch; ++c)
+    for (int m = 0; m < 4; ++m)
+      for (int jq = 0; jq < KC / 4; ++jq)
+        for (int n = 0; n < N; ++n)
+          for (int i = 0; i < 4; ++i) {
+            const int q = c * KC + 4 * jq + i, p = n / 16, k = n % 16;
+            if (q >= P || k >= M) continue;
+            const double x = A[((size_t)p * P + q) * 2 * K + (m < 2 ? 0 : K) + k];
+            const float hi = tf32_round((float)x);
+            B[((((size_t)c * 4 + m) * (KC / 4) + jq) * N + n) * 4 + i] = (m & 1) ? (float)(x - (double)hi) : hi;
+          }
+  return B;
+}
+
 // Build the dense contraction form for this solve? When its term count is above half
 // the dense matrix's size (M^2 P) the register-blocked product does less work than the
 // term loop. MMP_DENSE=0 / 1 forces the choice (M <= 16 either way).
@@ -911,6 +953,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));    // H
   off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);                // Raman tile carries
   off = align_up(off + (dense_wanted(b, s) ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));  // dense form
+  off = align_up(off + (dense_wanted(b, s) && !b->fp64 ? tc_floats(M, P) * sizeof(float) : 0));  // tensor-core form
   off = align_up(off + s.poly.size() * sizeof(double));
   off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -972,6 +1015,8 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_rt = off; off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);
   s.dense_ok = dense_wanted(b, s);
   const size_t o_dq = off; off = align_up(off + (s.dense_ok ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));
+  const bool tc_ok = s.dense_ok && !b->fp64;
+  const size_t o_tc = off; off = align_up(off + (tc_ok ? tc_floats(M, P) * sizeof(float) : 0));
   const size_t o_poly = off; off = align_up(off + s.poly.size() * sizeof(double));
   const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
@@ -1010,6 +1055,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
   d.raman_tiles = b->raman ? T2ptr(s.block, o_rt) : nullptr;
   d.dense_q = s.dense_ok ? T2ptr(s.block, o_dq) : nullptr;
+  d.dense_tc = tc_ok ? (const float*)T2ptr(s.block, o_tc) : nullptr;
   d.pairs = (const int2*)T2ptr(s.block, o_pairs);
   d.terms = (const Term*)T2ptr(s.block, o_terms);
   d.term_off = (const int*)T2ptr(s.block, o_toff);
@@ -1057,7 +1103,10 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
     } else {
       std::vector<float> Af(A.begin(), A.end());
       CUDA_TRY(cudaMemcpyAsync((void*)d.dense_q, Af.data(), n * sizeof(float), cudaMemcpyHostToDevice, b->stream));
-      CUDA_TRY(cudaStreamSynchronize(b->stream));  // Af is a host temporary
+      const std::vector<float> B = tc_operand(A, (int)M, (int)P);
+      CUDA_TRY(cudaMemcpyAsync((void*)d.dense_tc, B.data(), B.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               b->stream));
+      CUDA_TRY(cudaStreamSynchronize(b->stream));  // Af and B are host temporaries
     }
   }
   if (b->raman) {
@@ -1100,6 +1149,7 @@ bool batch_shape(mmp_batch* b) {
   size_t max_terms = 0;
   bool iir = b->raman;
   bool all_dense = true, any_dense = false;
+  int Mmin = 1 << 30;
   for (size_t i = 0; i < b->members.size(); ++i) {
     if (!b->active[i]) continue;
     const Member& s = b->members[i];
@@ -1108,6 +1158,7 @@ bool batch_shape(mmp_batch* b) {
     any_dense = any_dense || s.dense_ok;
     span = (uint32_t)i + 1;
     Mmax = std::max(Mmax, (int)s.M);
+    Mmin = std::min(Mmin, (int)s.M);
     Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
     Pall = std::max(Pall, (int)s.pairs.size());
     max_terms = std::max(max_terms, s.terms.size());
@@ -1127,17 +1178,36 @@ bool batch_shape(mmp_batch* b) {
   bool fused = iir && TT >= 64 && (int)b->nt >= TT;
   if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
     if (std::atoi(env) == 0) fused = false;
-  const int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
-  if (dense) smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
+  int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
+  // FP32 batches whose every solve has the dense form with at least kTcMinModes modes run
+  // it on the tensor cores (k_contract_tc, tiles of kTcTile samples) when the pair fields
+  // come from inside the tile or from U alone (Raman off); MMP_TC=0 keeps the
+  // register-blocked form. A batch that mixes in any other solve keeps the latter for all.
+  bool tc = !b->fp64 && span > 0 && all_dense && Mmin >= kTcMinModes && (int)b->nt >= kTcTile &&
+            (!b->raman || iir);
+  if (const char* env = std::getenv("MMP_TC"))
+    if (std::atoi(env) == 0) tc = false;
+  if (const char* env = std::getenv("MMP_RAMAN_FUSED"))  // the kernel forms the Raman fields itself
+    if (std::atoi(env) == 0 && b->raman) tc = false;
+  if (tc) {
+    TT = kTcTile;
+    fused = b->raman;
+    dense = 1;
+    smem = ((size_t)Mmax * TT + (size_t)kTcChunk * TT) * sizeof(float2) +
+           4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float);
+  } else if (dense) {
+    smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
+  }
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
   // are read through L1 from the FP64 table); the dense form reads no terms
   const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);
-  const int stage_terms = dense != 1 && smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
+  const int stage_terms = dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
   if (stage_terms) smem += max_terms * staged;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
                        stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
-                       fused != b->raman_fused || dense != b->dense;
+                       fused != b->raman_fused || dense != b->dense || tc != b->tc;
   b->dense = dense;
+  b->tc = tc;
   b->raman_iir = iir;
   b->raman_fused = fused;
   b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
@@ -1217,6 +1287,7 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->raman_recurrence = b->raman_fused ? 2u : (b->raman_iir ? 1u : 0u);
   info->graph_branches = b->groups;
   info->dense_contraction = (b->dense == 1 || (b->dense == 2 && s.dense_ok)) ? 1u : 0u;
+  info->tensor_core_contraction = b->tc ? 1u : 0u;
 }
 
 }  // namespace

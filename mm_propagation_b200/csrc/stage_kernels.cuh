@@ -25,6 +25,7 @@
 #include <type_traits>
 
 #include "fft.cuh"
+#include "tc_sm100.cuh"
 
 namespace mmp {
 
@@ -975,16 +976,61 @@ template <typename T> struct TileScan {
 // distinct banks per quarter warp; mask 0 is the plain layout.
 __device__ __forceinline__ int wsw(int h, int mask) { return h ^ ((h >> 3) & mask); }
 
+// The recurrence through one pair field of a contraction tile, by one warp (TT = 32 c
+// samples, 64 <= TT <= 256): V = U_l conj(U_m) is written coalesced to row (pair positions
+// swizzled by wmask), each lane takes its c samples into registers, the lanes' aggregates
+// are scanned, every lane runs the recurrence from the state entering it (carry[0..1]: the
+// states entering the tile for Re V and Im V) and W = (1 - f_R) V + R goes back in place.
 template <typename T>
-__device__ __forceinline__ void stage_u_tile(c2<T>* sU, const SolveDesc& d, int nt, int t0, int TT) {
-  const c2<T>* U = as_t2<T>(d.U);
-  const int H = TT >> 1;
-  for (int idx = threadIdx.x; idx < d.M * H; idx += blockDim.x) {
-    const int r = idx / H, tt = 2 * (idx - r * H);
-    c2<T> a, b;
-    ld2<T>(U + (size_t)r * nt + t0 + tt, a, b);
-    st2<T>(sU + r * TT + tt, a, b);
+__device__ __forceinline__ void tile_pair_recurrence(const TileScan<T>& ts, const c2<T>* sU, int TT, int2 lm,
+                                                     c2<T>* row, int wmask, const c2<T>* carry, T kerr,
+                                                     int lane) {
+  using V = c2<T>;
+  const int H = TT >> 1, c = ts.c, g = c >> 1;
+  // V = U_l conj(U_m), coalesced over the sample pairs
+  for (int h = lane; h < H; h += 32) {
+    V ul0, ul1, um0, um1;
+    ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
+    ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
+    st2<T>(row + 2 * wsw(h, wmask), cmulc(ul0, um0), cmulc(ul1, um1));
   }
+  __syncwarp();
+  V x[8];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (j < g) ld2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+  // this lane's aggregate from a zero start: sum_k lambda^(c-1-k) x_k, x_k = Re or Im V
+  V la = mk<T>(0, 0), lb = mk<T>(0, 0);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k < c) {
+      la = mk<T>(fma(ts.rw[k].x, x[k].x, la.x), fma(ts.rw[k].y, x[k].x, la.y));
+      lb = mk<T>(fma(ts.rw[k].x, x[k].y, lb.x), fma(ts.rw[k].y, x[k].y, lb.y));
+    }
+  }
+  ts.lane_scan(la, lb, lane);
+  // state entering this lane's samples: lambda^(c lane) C_tile + earlier lanes
+  V ea, eb;
+  ea.x = __shfl_up_sync(0xffffffffu, la.x, 1);
+  ea.y = __shfl_up_sync(0xffffffffu, la.y, 1);
+  eb.x = __shfl_up_sync(0xffffffffu, lb.x, 1);
+  eb.y = __shfl_up_sync(0xffffffffu, lb.y, 1);
+  if (lane == 0) ea = eb = mk<T>(0, 0);
+  V sa = cadd(cmul(ts.lane_pow, carry[0]), ea);
+  V sb = cadd(cmul(ts.lane_pow, carry[1]), eb);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k < c) {
+      sa = ts.step(sa, x[k].x);
+      sb = ts.step(sb, x[k].y);
+      // R = Im(kappa S), W = (1 - f_R) V + R
+      x[k] = mk<T>(fma(kerr, x[k].x, fma(ts.kt.x, sa.y, ts.kt.y * sa.x)),
+                   fma(kerr, x[k].y, fma(ts.kt.x, sb.y, ts.kt.y * sb.x)));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (j < g) st2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
 }
 
 template <typename T>
@@ -993,15 +1039,28 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SolveDesc& d = descs[blockIdx.y];
   const int tile = blockIdx.x, t0 = tile * TT;
-  if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;
+  if (t0 >= nt || d.M == 0) return;  // empty slot
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  V* sU = reinterpret_cast<V*>(smem_raw);
+  V* wt = sU + (size_t)d.M * TT;
+  {  // the U tile as 16-byte asynchronous copies, issued before the step check
+    const V* U = as_t2<T>(d.U);
+    const int per_row = TT * (int)sizeof(V) / 16;
+    for (int idx = threadIdx.x; idx < d.M * per_row; idx += blockDim.x) {
+      const int r = idx / per_row, c = idx - r * per_row;
+      cp_async16(reinterpret_cast<char*>(sU + (size_t)r * TT) + 16 * c,
+                 reinterpret_cast<const char*>(U + (size_t)r * nt + t0) + 16 * c);
+    }
+    cp_async_commit();
+  }
+  if (__ldcg(d.step) >= d.step_limit) {  // finished solve: the copies land before the CTA leaves
+    cp_async_wait<0>();
+    return;
+  }
   // The aggregate over the tile from a zero start is a weighted sum,
   //   S_end = sum_t lambda^(TT-1-t) x_t   (x = Re or Im of U_l conj(U_m)),
   // so it needs no sequential pass: the weights sit in a table, each lane sums its
   // samples (32 apart, coalesced) and the warp adds the lanes.
-  V* sU = reinterpret_cast<V*>(smem_raw);
-  V* wt = sU + (size_t)d.M * TT;
-  stage_u_tile<T>(sU, d, nt, t0, TT);
   for (int t = threadIdx.x; t < TT; t += blockDim.x) {  // lambda^(TT-1-t), FP64 powers
     double2 r = make_double2(1.0, 0.0), b = d.iir_lambda;
     for (int e = TT - 1 - t; e; e >>= 1) {
@@ -1010,6 +1069,7 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
     }
     wt[t] = from_d2<T>(r);
   }
+  cp_async_wait<0>();
   __syncthreads();
   const int ntiles = nt / TT;
   V* out = as_t2<T>(d.raman_tiles);
@@ -1112,6 +1172,12 @@ template <> __device__ __forceinline__ void lds16<double>(const double* a, doubl
   }
 }
 
+// Resident CTAs per SM the FP32 build is held to (registers): 3 for the term loop, 2 for the
+// dense form (its accumulators), none for FP64.
+template <typename T, int DENSE> constexpr int contract_min_blocks() {
+  return sizeof(T) == 4 ? (DENSE == 0 ? 3 : 2) : 1;
+}
+
 // raman_mode: 0 Raman off; 1 the convolutions R arrive as rows (k_pair / k_raman_scan);
 // 2 the recurrence runs through the tile here from the carries of k_raman_carry.
 // DENSE = 1: the contraction in its dense form (SolveDesc::dense_q, M <= 16, TT >= 64);
@@ -1122,7 +1188,7 @@ template <> __device__ __forceinline__ void lds16<double>(const double* a, doubl
 // one warp per (p, 64 samples), each lane two samples with all k in registers: a
 // register-blocked matrix product instead of one complex triple product per term.
 template <typename T, int DENSE>
-__global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
+__global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_contract(const SolveDesc* __restrict__ descs, int nt, int TT,
                                                   int stage_terms, int raman_mode) {
   using V = c2<T>;
   using ST = StagedTerm<T>;
@@ -1131,11 +1197,28 @@ __global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const Solv
   V* sU = reinterpret_cast<V*>(smem_raw);
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TT;
-  if (t0 >= nt || d.M == 0 || __ldcg(d.step) >= d.step_limit) return;  // empty slot / finished
+  if (t0 >= nt || d.M == 0) return;  // empty slot
   const int M = d.M;
   const int raman = raman_mode;
   const int P = d.P;                          // pair fields formed in this tile
   const int Pl = raman == 1 ? P : 0;          // pair rows loaded (Raman convolutions)
+  // The tile's rows are requested first, before the step check and the term staging
+  const V* U = as_t2<T>(d.U);
+  const V* R = as_t2<T>(d.W);
+  const unsigned row_bytes = (unsigned)(TT * sizeof(V));
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, (unsigned)(M + Pl) * row_bytes);
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M + Pl; r += blockDim.x) {
+    const V* src = (r < M) ? U + (size_t)r * nt + t0 : R + (size_t)(r - M) * nt + t0;
+    bulk_g2s(sU + (size_t)r * TT, src, row_bytes, &bar);
+  }
+  if (__ldcg(d.step) >= d.step_limit) {  // finished solve: the copies land before the CTA leaves
+    mbar_wait(&bar, 0, kMaxWaitPolls);
+    return;
+  }
   const T kerr = (T)d.one_minus_fR;
   V* sW = sU + (size_t)M * TT;
   const int n_terms = d.term_off[M];
@@ -1154,18 +1237,6 @@ __global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const Solv
       s.q = (T)tm.q;
       st[j] = s;
     }
-  }
-  const V* U = as_t2<T>(d.U);
-  const V* R = as_t2<T>(d.W);
-  const unsigned row_bytes = (unsigned)(TT * sizeof(V));
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, (unsigned)(M + Pl) * row_bytes);
-  }
-  __syncthreads();
-  for (int r = threadIdx.x; r < M + Pl; r += blockDim.x) {
-    const V* src = (r < M) ? U + (size_t)r * nt + t0 : R + (size_t)(r - M) * nt + t0;
-    bulk_g2s(sU + (size_t)r * TT, src, row_bytes, &bar);
   }
   // every thread polls with a bound; the barrier makes the outcome CTA-uniform and
   // also publishes the staged terms
@@ -1198,58 +1269,11 @@ __global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const Solv
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     TileScan<T> ts;
     ts.init(d, TT >> 5, lane);
-    const int c = ts.c, g = c >> 1;  // samples and sample pairs per lane (TT >= 64)
     const int ntiles = nt / TT;
     const V* tiles = as_t2<T>(d.raman_tiles);
-    for (int q = warp; q < P; q += nwarps) {
-      const int2 lm = d.pairs[q];
-      V* row = sW + (size_t)q * TT;
-      // V = U_l conj(U_m), coalesced over the sample pairs
-      for (int h = lane; h < H; h += 32) {
-        V ul0, ul1, um0, um1;
-        ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
-        ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
-        st2<T>(row + 2 * wsw(h, wmask), cmulc(ul0, um0), cmulc(ul1, um1));
-      }
-      __syncwarp();
-      V x[8];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < g) ld2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
-      // this lane's aggregate from a zero start: sum_k lambda^(c-1-k) x_k, x_k = Re or Im V
-      V la = mk<T>(0, 0), lb = mk<T>(0, 0);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (k < c) {
-          la = mk<T>(fma(ts.rw[k].x, x[k].x, la.x), fma(ts.rw[k].y, x[k].x, la.y));
-          lb = mk<T>(fma(ts.rw[k].x, x[k].y, lb.x), fma(ts.rw[k].y, x[k].y, lb.y));
-        }
-      }
-      ts.lane_scan(la, lb, lane);
-      // state entering this lane's samples: lambda^(c lane) C_tile + earlier lanes
-      V ea, eb;
-      ea.x = __shfl_up_sync(0xffffffffu, la.x, 1);
-      ea.y = __shfl_up_sync(0xffffffffu, la.y, 1);
-      eb.x = __shfl_up_sync(0xffffffffu, lb.x, 1);
-      eb.y = __shfl_up_sync(0xffffffffu, lb.y, 1);
-      if (lane == 0) ea = eb = mk<T>(0, 0);
-      const size_t ti = ((size_t)q * ntiles + blockIdx.x) * 2;
-      V sa = cadd(cmul(ts.lane_pow, tiles[ti]), ea);
-      V sb = cadd(cmul(ts.lane_pow, tiles[ti + 1]), eb);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (k < c) {
-          sa = ts.step(sa, x[k].x);
-          sb = ts.step(sb, x[k].y);
-          // R = Im(kappa S), W = (1 - f_R) V + R
-          x[k] = mk<T>(fma(kerr, x[k].x, fma(ts.kt.x, sa.y, ts.kt.y * sa.x)),
-                       fma(kerr, x[k].y, fma(ts.kt.x, sb.y, ts.kt.y * sb.x)));
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < g) st2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
-    }
+    for (int q = warp; q < P; q += nwarps)
+      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)q * TT, wmask,
+                              tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
   }
   __syncthreads();
   // 2. contraction
@@ -1355,6 +1379,165 @@ __global__ void __launch_bounds__(256, DENSE == 0 ? 3 : 1) k_contract(const Solv
     }
     st2<T>(sigma + (size_t)p * nt + t0 + tt, mk<T>(ax0, ay0), mk<T>(ax1, ay1));
   }
+}
+
+// ---- k_contract_tc: the dense contraction on the tensor cores (FP32 solves, M <= 16) -----
+// Per tile of kTcTile = 128 samples the dense form is two real matrix products over the
+// pair fields q,
+//   T_re[t][(p, k)] = sum_q Re W_q(t) A_re[p][q][k],   T_im[t][(p, k)] = sum_q Im W_q(t) A_im[p][q][k],
+// followed by sigma_p(t) = sum_k U_k(t) (T_re + i T_im) (the k_contract<T, 1> arithmetic).
+// The products are tcgen05 TF32 MMAs: M = 128 samples (TMEM lane = sample), N = 16 M
+// columns (p, k) per product (Re in TMEM columns [0, N), Im in [256, 256 + N)), K = the pair
+// fields in chunks of kTcChunk = 16. Both operands are split x = hi + lo into TF32 parts
+// and every product is formed as hi hi + hi lo + lo hi with FP32 accumulation: relative
+// error about 2^-21 (plain TF32 would leave 2^-11). Per chunk, the warps build the chunk's
+// pair fields W in shared memory (the Raman recurrence through the tile, raman_mode 2, or
+// V = U_l conj(U_m), raman_mode 0), pack them into the MMA's operand layout, and the
+// chunk's split coefficients (SolveDesc::dense_tc) arrive by one bulk copy; one thread
+// issues the chunk's 12 MMAs and commits them to an mbarrier. Every wait is bounded: on a
+// timeout the CTA flags kStatusTimeout, waits once more for its MMAs and frees its TMEM.
+template <typename T>
+__global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restrict__ descs, int nt, int raman_mode) {
+  static_assert(sizeof(T) == 4, "TF32 operands come from FP32 solves");
+  using V = float2;
+  constexpr int TT = kTcTile, KC = kTcChunk, WMASK = TT / 64 - 1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long bar_u, bar_b, bar_m;
+  __shared__ uint32_t s_tmem;
+  const SolveDesc& d = descs[blockIdx.y];
+  const int t0 = blockIdx.x * TT;
+  if (t0 >= nt || d.M == 0) return;  // empty slot
+  const int M = d.M, P = d.P, N = 16 * M;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  V* sU = reinterpret_cast<V*>(smem_raw);                        // [M][TT]
+  V* sW = sU + (size_t)M * TT;                                   // [KC][TT], pair positions swizzled
+  float* sA = reinterpret_cast<float*>(sW + (size_t)KC * TT);    // [4][KC/4][TT][4]
+  float* sB = sA + 4 * KC * TT;                                  // [4][KC/4][N][4]
+  if (tid == 0) {
+    mbar_init(&bar_u, 1);
+    mbar_init(&bar_b, 1);
+    mbar_init(&bar_m, 1);
+    mbar_arrive_expect_tx(&bar_u, (unsigned)(M * TT * sizeof(V)));
+  }
+  __syncthreads();
+  if (tid < M) bulk_g2s(sU + (size_t)tid * TT, as_t2<float>(d.U) + (size_t)tid * nt + t0, TT * sizeof(V), &bar_u);
+  if (__ldcg(d.step) >= d.step_limit) {  // finished solve: the copies land before the CTA leaves
+    mbar_wait(&bar_u, 0, kMaxWaitPolls);
+    return;
+  }
+  if (warp == 0) {
+    tc::alloc(&s_tmem, 512);
+    tc::relinquish();
+  }
+  tc::fence_before_sync();
+  bool ok = __syncthreads_and(mbar_wait(&bar_u, 0, kMaxWaitPolls) ? 1 : 0);
+  tc::fence_after_sync();
+  const uint32_t tmem = s_tmem;
+  TileScan<float> ts;
+  if (raman_mode == 2) ts.init(d, TT >> 5, lane);
+  const int ntiles = nt / TT;
+  const V* tiles = as_t2<float>(d.raman_tiles);
+  const float kerr = (float)d.one_minus_fR;
+  const int nch = (P + KC - 1) / KC;
+  const unsigned bbytes = (unsigned)(4 * KC * N * sizeof(float));
+  const uint32_t idesc = tc::idesc_tf32(TT, N);
+  int committed = -1;  // last chunk whose MMAs were committed
+  for (int c = 0; c < nch && ok; ++c) {
+    // the previous chunk's MMAs have completed: both operand buffers are free
+    if (tid == 0) {
+      mbar_arrive_expect_tx(&bar_b, bbytes);
+      bulk_g2s(sB, d.dense_tc + (size_t)c * 4 * KC * N, bbytes, &bar_b);
+    }
+    for (int j = warp; j < KC; j += 8) {  // pair field q = c KC + j, one warp each
+      const int q = c * KC + j;
+      if (q >= P) continue;
+      V* row = sW + (size_t)j * TT;
+      if (raman_mode == 2) {
+        tile_pair_recurrence<float>(ts, sU, TT, d.pairs[q], row, WMASK,
+                                    tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
+      } else {
+        const int2 lm = d.pairs[q];
+        for (int h = lane; h < TT / 2; h += 32) {
+          V ul0, ul1, um0, um1;
+          ld2<float>(sU + lm.x * TT + 2 * h, ul0, ul1);
+          ld2<float>(sU + lm.y * TT + 2 * h, um0, um1);
+          st2<float>(row + 2 * wsw(h, WMASK), cmulc(ul0, um0), cmulc(ul1, um1));
+        }
+      }
+    }
+    __syncthreads();
+    // pack: sample t, pair fields 4 jq .. 4 jq + 3 of the chunk -> one 16-byte group in
+    // each of the four operand matrices (fields beyond P are zero)
+    for (int it = tid; it < (KC / 4) * TT; it += blockDim.x) {
+      const int jq = it / TT, t = it - jq * TT;
+      const int pos = 2 * wsw(t >> 1, WMASK) + (t & 1);
+      float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int j = 4 * jq + i;
+        const V w = (c * KC + j < P) ? sW[(size_t)j * TT + pos] : make_float2(0.f, 0.f);
+        rh[i] = tc::tf32_hi(w.x);
+        rl[i] = w.x - rh[i];
+        ih[i] = tc::tf32_hi(w.y);
+        il[i] = w.y - ih[i];
+      }
+      float4* a4 = reinterpret_cast<float4*>(sA) + (size_t)jq * TT + t;
+      a4[0] = make_float4(rh[0], rh[1], rh[2], rh[3]);
+      a4[KC * TT / 4] = make_float4(rl[0], rl[1], rl[2], rl[3]);
+      a4[2 * KC * TT / 4] = make_float4(ih[0], ih[1], ih[2], ih[3]);
+      a4[3 * KC * TT / 4] = make_float4(il[0], il[1], il[2], il[3]);
+    }
+    tc::fence_proxy_async();
+    ok = __syncthreads_and(mbar_wait(&bar_b, c & 1, kMaxWaitPolls) ? 1 : 0);
+    if (!ok) break;
+    tc::fence_after_sync();
+    if (tid == 0) {
+      // Re: (A Re hi, B Re hi), (Re hi, Re lo), (Re lo, Re hi); Im likewise
+      constexpr int ta[3] = {0, 0, 1}, tb[3] = {0, 1, 0};
+#pragma unroll
+      for (int part = 0; part < 2; ++part)
+#pragma unroll
+        for (int term = 0; term < 3; ++term)
+#pragma unroll
+          for (int ks = 0; ks < KC / 8; ++ks) {
+            const float* a = sA + (size_t)(2 * part + ta[term]) * KC * TT + ks * 2 * TT * 4;
+            const float* b = sB + (size_t)(2 * part + tb[term]) * KC * N + ks * 2 * N * 4;
+            tc::mma_tf32(tmem + 256u * part, tc::desc_kmajor(a, TT * 16, 128), tc::desc_kmajor(b, N * 16, 128),
+                         idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
+          }
+      tc::commit(&bar_m);
+    }
+    committed = c;
+    ok = __syncthreads_and(mbar_wait(&bar_m, c & 1, kMaxWaitPolls) ? 1 : 0);
+    tc::fence_after_sync();
+  }
+  if (ok) {
+    // sigma_p(t) = sum_k U_k(t) (T_re + i T_im): warp w reads TMEM lanes 32 (w % 4) .. + 31
+    const int quad = warp & 3, t = quad * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
+    V* sigma = as_t2<float>(d.sigma);
+    for (int p = warp >> 2; p < M; p += 2) {
+      float re[16], im[16];
+      tc::ld16(tl + 16u * p, re);
+      tc::ld16(tl + 256u + 16u * p, im);
+      float sx = 0.f, sy = 0.f;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k < M) {
+          const V u = sU[k * TT + t];
+          sx = fmaf(u.x, re[k], fmaf(-u.y, im[k], sx));
+          sy = fmaf(u.x, im[k], fmaf(u.y, re[k], sy));
+        }
+      }
+      sigma[(size_t)p * nt + t0 + t] = make_float2(sx, sy);
+    }
+  } else {
+    if (tid == 0) atomicOr(d.status, kStatusTimeout);
+    if (committed >= 0) mbar_wait(&bar_m, committed & 1, kMaxWaitPolls);  // MMAs still in flight
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::dealloc(tmem, 512);
 }
 
 // FP64 rows -> T rows (used for the Raman spectrum)

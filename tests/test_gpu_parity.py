@@ -238,3 +238,44 @@ def test_fp32_monitors_match_fp64(mmp):
     assert len(e32) == len(p32) == 100 and p64.min() > 0
     assert np.abs(e32 / e64 - 1).max() < 1e-6
     assert np.abs(p32 / p64 - 1).max() < 1e-5
+
+
+def _dense_case(seed, M, nt, n_steps, raman):
+    prob = W.dense15(seed=seed, M=M, nt=nt, n_steps=n_steps, raman=raman)
+    return W.scale_power(prob, W.phase_cap_scale(prob, per_step=0.05, total=0.3))
+
+
+@pytest.mark.parametrize("raman", [True, False])
+def test_dense_contraction_on_tensor_cores(mmp, monkeypatch, raman):
+    # fully symmetric Q at M = 8 (36 pair fields: two full K chunks of 16 and a partial
+    # one): the tensor-core form (TF32 operands split hi + lo, FP32 sums) against the
+    # register-blocked FP32 form and the oracle
+    prob = _dense_case(94, 8, 1024, 6, raman)
+    out_t, info_t = run(mmp, prob, [6])
+    monkeypatch.setenv("MMP_TC", "0")
+    out_s, info_s = run(mmp, prob, [6])
+    assert (info_t["tensor_core_contraction"], info_s["tensor_core_contraction"]) == (1, 0)
+    assert info_t["dense_contraction"] == info_s["dense_contraction"] == 1
+    assert mo.rel_l2_per_mode(out_t, out_s).max() < 2e-6
+    assert mo.rel_l2_per_mode(out_t, mo.solve(prob)).max() < TOL32
+
+
+def test_dense_contraction_on_tensor_cores_15_modes(mmp, monkeypatch):
+    # the dense 15-mode workload's shape: 120 pair fields in 8 K chunks, N = 240 columns
+    prob = _dense_case(95, 15, 1024, 4, True)
+    out_t, info_t = run(mmp, prob, [4])
+    monkeypatch.setenv("MMP_TC", "0")
+    out_s, _ = run(mmp, prob, [4])
+    assert info_t["tensor_core_contraction"] == 1
+    assert mo.rel_l2_per_mode(out_t, out_s).max() < 2e-6
+
+
+def test_tensor_core_batch_members_match_single_solves(mmp):
+    # solves of different M in one batch: each tile's MMA shape comes from its own solve
+    probs = [_dense_case(96 + i, m, 512, 5, True) for i, m in enumerate([6, 8, 7])]
+    singles = [run(mmp, p, [5])[0] for p in probs]
+    with mmp.Batch(probs) as b:
+        b.propagate(5)
+        assert b.info(0)["tensor_core_contraction"] == 1
+        for i in range(len(probs)):
+            assert np.array_equal(b.result(i), singles[i]), i
