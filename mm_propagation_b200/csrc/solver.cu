@@ -161,7 +161,7 @@ int ensure_device(int dev, DeviceRes** out) {
   for (const void* f : contract_fns)
     CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                200 * 1024));
+                                224 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
@@ -577,7 +577,7 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
                        (const void*)&k_contract<double, 2>};
   if (b->tc) {
     void* targs[] = {(void*)&descs, &nt, &mode};
-    CUDA_TRY(launch((const void*)&k_contract_tc<float>, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, targs));
+    CUDA_TRY(launch((const void*)&k_contract_tc<float>, grid, 512, (int)b->contract_smem, 1, st ? st : b->stream, targs));
     return MMP_OK;
   }
   const void* fn = b->fp64 ? f64[b->dense] : f32[b->dense];
@@ -1194,7 +1194,7 @@ bool batch_shape(mmp_batch* b) {
     fused = b->raman;
     dense = 1;
     smem = ((size_t)Mmax * TT + (size_t)kTcChunk * TT) * sizeof(float2) +
-           4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float);
+           2 * 4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float);  // two operand buffers
   } else if (dense) {
     smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
   }

@@ -1390,33 +1390,37 @@ __global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_cont
 // columns (p, k) per product (Re in TMEM columns [0, N), Im in [256, 256 + N)), K = the pair
 // fields in chunks of kTcChunk = 16. Both operands are split x = hi + lo into TF32 parts
 // and every product is formed as hi hi + hi lo + lo hi with FP32 accumulation: relative
-// error about 2^-21 (plain TF32 would leave 2^-11). Per chunk, the warps build the chunk's
-// pair fields W in shared memory (the Raman recurrence through the tile, raman_mode 2, or
-// V = U_l conj(U_m), raman_mode 0), pack them into the MMA's operand layout, and the
-// chunk's split coefficients (SolveDesc::dense_tc) arrive by one bulk copy; one thread
-// issues the chunk's 12 MMAs and commits them to an mbarrier. Every wait is bounded: on a
-// timeout the CTA flags kStatusTimeout, waits once more for its MMAs and frees its TMEM.
+// error about 2^-21 (plain TF32 would leave 2^-11).
+// Per chunk c the 16 warps build the chunk's pair fields W in shared memory, one field each
+// (the Raman recurrence through the tile, raman_mode 2, or V = U_l conj(U_m), raman_mode 0),
+// pack them into the MMA's operand layout (buffer c % 2), and one thread issues the chunk's
+// 12 MMAs and commits them to an mbarrier; the chunk's split coefficients
+// (SolveDesc::dense_tc) arrive by one bulk copy issued when the chunk starts. The MMAs of
+// chunk c run while the warps build chunk c + 1. Every wait is bounded: on a timeout the
+// CTA flags kStatusTimeout, waits once more for its MMAs and frees its TMEM.
 template <typename T>
-__global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restrict__ descs, int nt, int raman_mode) {
+__global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restrict__ descs, int nt, int raman_mode) {
   static_assert(sizeof(T) == 4, "TF32 operands come from FP32 solves");
   using V = float2;
   constexpr int TT = kTcTile, KC = kTcChunk, WMASK = TT / 64 - 1;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) unsigned long long bar_u, bar_b, bar_m;
+  __shared__ __align__(8) unsigned long long bar_u, bar_b[2], bar_m[2];
   __shared__ uint32_t s_tmem;
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TT;
   if (t0 >= nt || d.M == 0) return;  // empty slot
   const int M = d.M, P = d.P, N = 16 * M;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   V* sU = reinterpret_cast<V*>(smem_raw);                        // [M][TT]
   V* sW = sU + (size_t)M * TT;                                   // [KC][TT], pair positions swizzled
-  float* sA = reinterpret_cast<float*>(sW + (size_t)KC * TT);    // [4][KC/4][TT][4]
-  float* sB = sA + 4 * KC * TT;                                  // [4][KC/4][N][4]
+  float* sA = reinterpret_cast<float*>(sW + (size_t)KC * TT);    // [2][4][KC/4][TT][4]
+  float* sB = sA + 2 * 4 * KC * TT;                              // [2][4][KC/4][N][4]
   if (tid == 0) {
     mbar_init(&bar_u, 1);
-    mbar_init(&bar_b, 1);
-    mbar_init(&bar_m, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&bar_b[i], 1);
+      mbar_init(&bar_m[i], 1);
+    }
     mbar_arrive_expect_tx(&bar_u, (unsigned)(M * TT * sizeof(V)));
   }
   __syncthreads();
@@ -1443,12 +1447,19 @@ __global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restr
   const uint32_t idesc = tc::idesc_tf32(TT, N);
   int committed = -1;  // last chunk whose MMAs were committed
   for (int c = 0; c < nch && ok; ++c) {
-    // the previous chunk's MMAs have completed: both operand buffers are free
-    if (tid == 0) {
-      mbar_arrive_expect_tx(&bar_b, bbytes);
-      bulk_g2s(sB, d.dense_tc + (size_t)c * 4 * KC * N, bbytes, &bar_b);
+    const int buf = c & 1;
+    float* A = sA + (size_t)buf * 4 * KC * TT;
+    float* B = sB + (size_t)buf * 4 * KC * N;
+    if (c >= 2) {  // chunk c - 2's MMAs read this buffer pair: wait for them
+      ok = __syncthreads_and(mbar_wait(&bar_m[buf], ((c - 2) >> 1) & 1, kMaxWaitPolls) ? 1 : 0);
+      if (!ok) break;
+      tc::fence_after_sync();
     }
-    for (int j = warp; j < KC; j += 8) {  // pair field q = c KC + j, one warp each
+    if (tid == 0) {
+      mbar_arrive_expect_tx(&bar_b[buf], bbytes);
+      bulk_g2s(B, d.dense_tc + (size_t)c * 4 * KC * N, bbytes, &bar_b[buf]);
+    }
+    for (int j = warp; j < KC; j += nwarps) {  // pair field q = c KC + j, one warp each
       const int q = c * KC + j;
       if (q >= P) continue;
       V* row = sW + (size_t)j * TT;
@@ -1481,14 +1492,16 @@ __global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restr
         ih[i] = tc::tf32_hi(w.y);
         il[i] = w.y - ih[i];
       }
-      float4* a4 = reinterpret_cast<float4*>(sA) + (size_t)jq * TT + t;
+      float4* a4 = reinterpret_cast<float4*>(A) + (size_t)jq * TT + t;
       a4[0] = make_float4(rh[0], rh[1], rh[2], rh[3]);
       a4[KC * TT / 4] = make_float4(rl[0], rl[1], rl[2], rl[3]);
       a4[2 * KC * TT / 4] = make_float4(ih[0], ih[1], ih[2], ih[3]);
       a4[3 * KC * TT / 4] = make_float4(il[0], il[1], il[2], il[3]);
     }
     tc::fence_proxy_async();
-    ok = __syncthreads_and(mbar_wait(&bar_b, c & 1, kMaxWaitPolls) ? 1 : 0);
+    // the chunk's coefficients have landed and every thread's operand writes are done
+    // (sW is free again for the next chunk once this barrier is passed)
+    ok = __syncthreads_and(mbar_wait(&bar_b[buf], (c >> 1) & 1, kMaxWaitPolls) ? 1 : 0);
     if (!ok) break;
     tc::fence_after_sync();
     if (tid == 0) {
@@ -1500,23 +1513,25 @@ __global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restr
         for (int term = 0; term < 3; ++term)
 #pragma unroll
           for (int ks = 0; ks < KC / 8; ++ks) {
-            const float* a = sA + (size_t)(2 * part + ta[term]) * KC * TT + ks * 2 * TT * 4;
-            const float* b = sB + (size_t)(2 * part + tb[term]) * KC * N + ks * 2 * N * 4;
+            const float* a = A + (size_t)(2 * part + ta[term]) * KC * TT + ks * 2 * TT * 4;
+            const float* b = B + (size_t)(2 * part + tb[term]) * KC * N + ks * 2 * N * 4;
             tc::mma_tf32(tmem + 256u * part, tc::desc_kmajor(a, TT * 16, 128), tc::desc_kmajor(b, N * 16, 128),
                          idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
           }
-      tc::commit(&bar_m);
+      tc::commit(&bar_m[buf]);
     }
     committed = c;
-    ok = __syncthreads_and(mbar_wait(&bar_m, c & 1, kMaxWaitPolls) ? 1 : 0);
-    tc::fence_after_sync();
   }
+  // the last chunk's MMAs complete after all earlier ones (in-order issue, one thread)
+  if (ok && committed >= 0)
+    ok = __syncthreads_and(mbar_wait(&bar_m[committed & 1], (committed >> 1) & 1, kMaxWaitPolls) ? 1 : 0);
+  tc::fence_after_sync();
   if (ok) {
     // sigma_p(t) = sum_k U_k(t) (T_re + i T_im): warp w reads TMEM lanes 32 (w % 4) .. + 31
     const int quad = warp & 3, t = quad * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
     V* sigma = as_t2<float>(d.sigma);
-    for (int p = warp >> 2; p < M; p += 2) {
+    for (int p = warp >> 2; p < M; p += nwarps >> 2) {
       float re[16], im[16];
       tc::ld16(tl + 16u * p, re);
       tc::ld16(tl + 256u + 16u * p, im);
@@ -1533,7 +1548,7 @@ __global__ void __launch_bounds__(256, 1) k_contract_tc(const SolveDesc* __restr
     }
   } else {
     if (tid == 0) atomicOr(d.status, kStatusTimeout);
-    if (committed >= 0) mbar_wait(&bar_m, committed & 1, kMaxWaitPolls);  // MMAs still in flight
+    if (committed >= 0) mbar_wait(&bar_m[committed & 1], (committed >> 1) & 1, kMaxWaitPolls);  // MMAs in flight
   }
   tc::fence_before_sync();
   __syncthreads();
