@@ -262,6 +262,27 @@ def stage_flops(prob, pairs, n_terms, raman_path):
     return {"pair": pair, "contract": contract, "nu": nu}
 
 
+def tc_mma_flops(prob, pairs):
+    """TF32 work the tensor-core contraction issues per solve and launch: per tile of 128
+    samples and chunk of 16 pair fields, 2 products (Re, Im) x 3 split terms (hi hi, hi lo,
+    lo hi) of 128 x 16 M x 16 MMA work, i.e. 2 * 3 * 2 * 16 ceil(P/16) * 16 M flops per sample."""
+    chunks = -(-pairs // 16)
+    return 2 * 3 * 2.0 * 16 * chunks * 16 * prob.n_modes * prob.nt
+
+
+def tf32_peak_tflops():
+    """Dense TF32 tensor peak: the measured BF16 burst (MEASURED_PEAKS.json bf16_tflops)
+    halved, TF32 MMAs running at half the BF16 rate on this part (nominal 1.1 vs 2.25
+    PFLOP/s); 1.1 PFLOP/s nominal when no measurement is present."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if d.get("bf16_tflops"):
+            return float(d["bf16_tflops"]) / 2, "measured BF16 burst (MEASURED_PEAKS.json bf16_tflops) / 2"
+    return 1100.0, "nominal dense TF32"
+
+
 def fp32_peak_tflops():
     """Nominal FP32 (non-tensor) peak: 148 SMs x 128 lanes x 2 flops x max SM clock.
     MEASURED_PEAKS.json carries no FP32 figure."""
@@ -428,8 +449,9 @@ def ours_arm(args, dist):
     n_terms = int((probe.coupling["value"] != 0).sum())
     per = stage_bytes(probe, tab[3], tab[0], tab[1], bt, n_pairs, raman_path)
     flops = stage_flops(probe, n_pairs, n_terms, raman_path)
+    tc = bool(info.get("tensor_core_contraction", 0))
     names = {"pair": ("k_pair", "k_raman_scan", "k_raman_agg+k_raman_carry")[raman_path],
-             "contract": "k_contract", "nu": "k_nu"}
+             "contract": "k_contract_tc" if tc else "k_contract", "nu": "k_nu"}
     share = {k: prof[k]["ms_per_launch"] * prof[k]["launches"] for k in prof}
     tot = sum(share.values())
     dom = max(share, key=share.get)
@@ -450,14 +472,31 @@ def ours_arm(args, dist):
                       "fp32_frac": flops_launch / t / 1e12 / fpeak,
                       "roofline_bound": "hbm" if t_hbm >= t_fp32 else "fp32",
                       "roofline_frac": max(t_hbm, t_fp32) / t}
+    tpeak, tpeak_src = tf32_peak_tflops()
+    if tc and "contract" in kernels:
+        # the dense contraction on the tensor cores: its issued TF32 MMA work against the TF32 peak
+        kc = kernels["contract"]
+        tflops = tc_mma_flops(probe, n_pairs) * args.batch
+        t = kc["ms_per_launch"] / 1e3
+        t_tensor = tflops / (tpeak * 1e12)
+        kc.update({"tensor_flops_per_launch": tflops, "achieved_tensor_tflops": tflops / t / 1e12,
+                   "tensor_frac": tflops / t / 1e12 / tpeak,
+                   "roofline_bound": "tensor" if t_tensor >= kc["alg_bytes_per_launch"] / (peak * 1e9) else "hbm",
+                   "roofline_frac": max(t_tensor, kc["alg_bytes_per_launch"] / (peak * 1e9)) / t})
     traffic_solve = read_ncu_traffic(names[dom].split("+")[0], args.workload)
-    roof = {"bound": "hbm", "kernel": names[dom],
-            "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-            "frac": kernels[dom]["frac"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic_solve * args.batch if traffic_solve else None,
-            "alg_bytes_per_launch": kernels[dom]["alg_bytes_per_launch"],
-            "fp32_peak_tflops": fpeak, "fp32_peak_source": "nominal: 148 SMs x 128 lanes x 2 x max SM clock",
-            "kernels": kernels}
+    if tc and dom == "contract":
+        kc = kernels["contract"]
+        roof = {"bound": "tensor", "kernel": names[dom], "achieved": kc["achieved_tensor_tflops"], "peak": tpeak,
+                "unit": "TFLOP/s", "frac": kc["tensor_frac"], "peak_source": tpeak_src,
+                "tensor_flops_per_launch": kc["tensor_flops_per_launch"]}
+    else:
+        roof = {"bound": "hbm", "kernel": names[dom], "achieved": kernels[dom]["achieved_gbs"], "peak": peak,
+                "unit": "GB/s", "frac": kernels[dom]["frac"],
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    roof.update({"traffic": traffic_solve * args.batch if traffic_solve else None,
+                 "alg_bytes_per_launch": kernels[dom]["alg_bytes_per_launch"],
+                 "fp32_peak_tflops": fpeak, "fp32_peak_source": "nominal: 148 SMs x 128 lanes x 2 x max SM clock",
+                 "kernels": kernels})
 
     # accuracy and the CPU baseline (rank 0, N=1 only)
     cpu = None
