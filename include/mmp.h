@@ -113,6 +113,8 @@ typedef struct mmp_info {
                                                product over (p, k) x pair fields (M <= 16) */
   uint32_t tensor_core_contraction;         /* 1: that dense product runs on the tensor cores
                                                (tcgen05, TF32 operands split hi + lo, FP32 sums) */
+  uint32_t contract_pair_chunk;             /* > 0: pair fields held per chunk by the contraction
+                                               of tall tiles (Raman recurrence in the tiles) */
 } mmp_info;
 
 typedef struct mmp_solver mmp_solver;

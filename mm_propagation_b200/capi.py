@@ -78,6 +78,7 @@ class mmp_info(C.Structure):
         ("graph_branches", C.c_uint32),
         ("dense_contraction", C.c_uint32),
         ("tensor_core_contraction", C.c_uint32),
+        ("contract_pair_chunk", C.c_uint32),
     ]
 
 

@@ -99,6 +99,8 @@ namespace {
 
 // shared memory of k_raman_scan: a 128 KB segment of V, padded
 constexpr int kScanSmem = padded_len(128 * 1024 / 8) * 8;
+// Dynamic shared memory k_contract may take (the 227 KB per block, less its static part)
+constexpr size_t kContractSmemMax = 226 * 1024;
 
 // ---- per-device resources: twiddle tables, kernel attributes ------------------------------
 struct DeviceRes {
@@ -159,7 +161,11 @@ int ensure_device(int dev, DeviceRes** out) {
                                 (const void*)&k_contract<float, 2>,  (const void*)&k_contract<double, 0>,
                                 (const void*)&k_contract<double, 1>, (const void*)&k_contract<double, 2>};
   for (const void* f : contract_fns)
-    CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kContractSmemMax));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_pc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                110 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_pc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                110 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 224 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
@@ -448,6 +454,10 @@ void host_setup(const mmp_params* p, Member& s) {
       t.q = e->value / max_Q;                                           // Q_tilde (:117-136)
       s.terms.push_back(t);
     }
+    // each p's terms in pair-field order (stable): the pair-chunked contraction walks
+    // them chunk by chunk with one cursor
+    std::stable_sort(s.terms.begin() + s.term_off[q], s.terms.end(),
+                     [](const Term& a, const Term& b) { return (a.pc & 0x7fff) < (b.pc & 0x7fff); });
   }
   s.term_off[M] = (int)s.terms.size();
 }
@@ -481,6 +491,7 @@ struct mmp_batch {
   bool raman_fused = false;  // ... and the recurrence runs inside the contraction tiles
   int dense = 0;  // contraction form: 0 term loop, 1 dense (k_contract<T, 1>), 2 per solve
   bool tc = false;  // dense form on the tensor cores (k_contract_tc)
+  int pchunk = 0;   // > 0: pair fields per chunk of the pair-chunked contraction (k_contract_pc)
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -575,6 +586,13 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
                        (const void*)&k_contract<float, 2>};
   const void* f64[] = {(const void*)&k_contract<double, 0>, (const void*)&k_contract<double, 1>,
                        (const void*)&k_contract<double, 2>};
+  if (b->pchunk) {
+    int pc = b->pchunk;
+    void* pargs[] = {(void*)&descs, &nt, &TT, &pc};
+    const void* fpc = b->fp64 ? (const void*)&k_contract_pc<double> : (const void*)&k_contract_pc<float>;
+    CUDA_TRY(launch(fpc, grid, 256, (int)b->contract_smem, 1, st ? st : b->stream, pargs));
+    return MMP_OK;
+  }
   if (b->tc) {
     void* targs[] = {(void*)&descs, &nt, &mode};
     CUDA_TRY(launch((const void*)&k_contract_tc<float>, grid, 512, (int)b->contract_smem, 1, st ? st : b->stream, targs));
@@ -1201,13 +1219,38 @@ bool batch_shape(mmp_batch* b) {
   // terms follow the tiles in shared memory, coefficient in T, when they fit (else they
   // are read through L1 from the FP64 table); the dense form reads no terms
   const size_t staged = b->fp64 ? sizeof(StagedTerm<double>) : sizeof(StagedTerm<float>);
-  const int stage_terms = dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0;
-  if (stage_terms) smem += max_terms * staged;
+  // Tall tiles (the U tile and every pair field do not fit at 64 samples or more): the
+  // pair-chunked contraction keeps the recurrence in the tiles with only a chunk of pair
+  // fields in shared memory (3 CTAs per SM in FP32, 2 in FP64), instead of the row scan
+  // writing P Raman rows to HBM for the contraction to read back. MMP_PAIR_CHUNK=0 keeps
+  // the row scan.
+  int pchunk = 0;
+  bool pc_ok = iir && !fused && !any_dense && span > 0;
+  if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
+    if (std::atoi(env) == 0) pc_ok = false;
+  if (const char* env = std::getenv("MMP_PAIR_CHUNK"))
+    if (std::atoi(env) == 0) pc_ok = false;
+  if (pc_ok) {
+    int tc_tt = 256;  // items per thread: M TT / 2 <= kPcItems * 256
+    while (tc_tt > 64 && (size_t)Mmax * tc_tt > 2 * kPcItems * 256) tc_tt >>= 1;
+    while (tc_tt > (int)b->nt) tc_tt >>= 1;
+    const size_t budget = b->fp64 ? 110 * 1024 : 72 * 1024;
+    const size_t fixed = (size_t)Mmax * tc_tt * t2 + max_terms * staged;
+    if (tc_tt >= 64 && (size_t)Mmax * tc_tt <= 2 * kPcItems * 256 && fixed + 8 * (size_t)tc_tt * t2 <= budget) {
+      pchunk = (int)std::min<size_t>((size_t)std::max(Pmax, 1), (budget - fixed) / ((size_t)tc_tt * t2));
+      TT = tc_tt;
+      fused = true;
+      smem = fixed + (size_t)pchunk * tc_tt * t2;
+    }
+  }
+  const int stage_terms = pchunk ? 1 : (dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0);
+  if (stage_terms && !pchunk) smem += max_terms * staged;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
                        stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
-                       fused != b->raman_fused || dense != b->dense || tc != b->tc;
+                       fused != b->raman_fused || dense != b->dense || tc != b->tc || pchunk != b->pchunk;
   b->dense = dense;
   b->tc = tc;
+  b->pchunk = pchunk;
   b->raman_iir = iir;
   b->raman_fused = fused;
   b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
@@ -1288,6 +1331,7 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->graph_branches = b->groups;
   info->dense_contraction = (b->dense == 1 || (b->dense == 2 && s.dense_ok)) ? 1u : 0u;
   info->tensor_core_contraction = b->tc ? 1u : 0u;
+  info->contract_pair_chunk = (uint32_t)b->pchunk;
 }
 
 }  // namespace

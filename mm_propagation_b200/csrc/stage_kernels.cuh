@@ -1381,6 +1381,117 @@ __global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_cont
   }
 }
 
+// ---- k_contract_pc: the term loop with the Raman recurrence in the tiles, for tiles with
+// too many pair fields to hold at once (tall tiles). Only `pc` pair fields live in shared
+// memory at a time: per chunk the warps run the recurrence for the chunk's fields, then
+// every thread advances each of its (p, two samples) items through the terms of p whose
+// pair field lies in the chunk, accumulating in registers. The terms of each p are sorted
+// by pair field, so one cursor per item walks them chunk by chunk. At most kPcItems items
+// per thread (M * TT / 2 <= kPcItems * blockDim.x), every term staged in shared memory.
+constexpr int kPcItems = 4;
+template <typename T>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(const SolveDesc* __restrict__ descs,
+                                                                              int nt, int TT, int pc) {
+  using V = c2<T>;
+  using ST = StagedTerm<T>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long bar;
+  V* sU = reinterpret_cast<V*>(smem_raw);  // [M][TT]
+  const SolveDesc& d = descs[blockIdx.y];
+  const int t0 = blockIdx.x * TT;
+  if (t0 >= nt || d.M == 0) return;  // empty slot
+  const int M = d.M, P = d.P;
+  const unsigned row_bytes = (unsigned)(TT * sizeof(V));
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, (unsigned)M * row_bytes);
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M; r += blockDim.x)
+    bulk_g2s(sU + (size_t)r * TT, as_t2<T>(d.U) + (size_t)r * nt + t0, row_bytes, &bar);
+  if (__ldcg(d.step) >= d.step_limit) {  // finished solve: the copies land before the CTA leaves
+    mbar_wait(&bar, 0, kMaxWaitPolls);
+    return;
+  }
+  V* sW = sU + (size_t)M * TT;                             // [pc][TT], pair positions swizzled
+  ST* st = reinterpret_cast<ST*>(sW + (size_t)pc * TT);   // every term, sorted by (p, pair field)
+  const int n_terms = d.term_off[M];
+  for (int j = threadIdx.x; j < n_terms; j += blockDim.x) {
+    const Term tm = d.terms[j];
+    ST x;
+    x.k = tm.k;
+    x.pc = tm.pc;
+    x.q = (T)tm.q;
+    st[j] = x;
+  }
+  const bool landed = mbar_wait(&bar, 0, kMaxWaitPolls);
+  if (!__syncthreads_and(landed ? 1 : 0)) {
+    if (threadIdx.x == 0) atomicOr(d.status, kStatusTimeout);
+    mbar_wait(&bar, 0, kMaxWaitPolls);
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int H = TT >> 1, nitems = M * H;
+  const int wmask = max(TT >> 6, 1) - 1;
+  const T kerr = (T)d.one_minus_fR;
+  const int ntiles = nt / TT;
+  const V* tiles = as_t2<T>(d.raman_tiles);
+  TileScan<T> ts;
+  ts.init(d, TT >> 5, lane);
+  T acc[kPcItems][4];
+  int cur[kPcItems], end[kPcItems];
+#pragma unroll
+  for (int i = 0; i < kPcItems; ++i) {
+    const int idx = threadIdx.x + i * blockDim.x;
+    const int p = idx < nitems ? idx / H : 0;
+    cur[i] = idx < nitems ? d.term_off[p] : 0;
+    end[i] = idx < nitems ? d.term_off[p + 1] : 0;
+    acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0;
+  }
+  for (int c0 = 0; c0 < P; c0 += pc) {
+    const int c1 = min(P, c0 + pc);
+    for (int q = c0 + warp; q < c1; q += nwarps)
+      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)(q - c0) * TT, wmask,
+                              tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kPcItems; ++i) {
+      const int idx = threadIdx.x + i * blockDim.x;
+      if (idx >= nitems) continue;
+      const int p = idx / H, tt = 2 * (idx - p * H);
+      const int tw = 2 * wsw(tt >> 1, wmask);
+      int j = cur[i];
+      for (; j < end[i]; ++j) {
+        const ST x = st[j];
+        const int q = x.pc & 0x7fff;
+        if (q >= c1) break;
+        V u0, u1, w0, w1;
+        ld2<T>(sU + x.k * TT + tt, u0, u1);
+        ld2<T>(sW + (q - c0) * TT + tw, w0, w1);
+        if (x.pc & 0x8000) {
+          w0.y = -w0.y;
+          w1.y = -w1.y;
+        }
+        const V a0 = cmul(u0, w0), a1 = cmul(u1, w1);
+        acc[i][0] = fma(x.q, a0.x, acc[i][0]);
+        acc[i][1] = fma(x.q, a0.y, acc[i][1]);
+        acc[i][2] = fma(x.q, a1.x, acc[i][2]);
+        acc[i][3] = fma(x.q, a1.y, acc[i][3]);
+      }
+      cur[i] = j;
+    }
+    __syncthreads();  // the chunk's fields are read before the next chunk overwrites them
+  }
+  V* sigma = as_t2<T>(d.sigma);
+#pragma unroll
+  for (int i = 0; i < kPcItems; ++i) {
+    const int idx = threadIdx.x + i * blockDim.x;
+    if (idx >= nitems) continue;
+    const int p = idx / H, tt = 2 * (idx - p * H);
+    st2<T>(sigma + (size_t)p * nt + t0 + tt, mk<T>(acc[i][0], acc[i][1]), mk<T>(acc[i][2], acc[i][3]));
+  }
+}
+
 // ---- k_contract_tc: the dense contraction on the tensor cores (FP32 solves, M <= 16) -----
 // Per tile of kTcTile = 128 samples the dense form is two real matrix products over the
 // pair fields q,

@@ -279,3 +279,21 @@ def test_tensor_core_batch_members_match_single_solves(mmp):
         assert b.info(0)["tensor_core_contraction"] == 1
         for i in range(len(probs)):
             assert np.array_equal(b.result(i), singles[i]), i
+
+
+def test_raman_recurrence_in_tall_tiles(mmp, monkeypatch):
+    # over 200 pair fields (328 with the reference's pair-slot mapping): U and all pair
+    # fields do not fit in a 64-sample tile, so the contraction holds the pair fields in
+    # chunks (k_contract_pc) with the recurrence still in the tiles; against the row scan
+    # (Raman rows through HBM) and the oracle
+    prob = W.small_case(seed=97, M=26, nt=512, n_steps=3, nnz_target=1800)
+    for fl, tol in ((0, 2e-6), (capi.MMP_F_FP64, 1e-12)):
+        out_t, info_t = run(mmp, prob, [3], fl)
+        monkeypatch.setenv("MMP_PAIR_CHUNK", "0")
+        out_s, info_s = run(mmp, prob, [3], fl)
+        monkeypatch.delenv("MMP_PAIR_CHUNK")
+        assert (info_t["raman_recurrence"], info_s["raman_recurrence"]) == (2, 1)
+        assert info_t["n_pair_fields"] > 200
+        assert 0 < info_t["contract_pair_chunk"] < info_t["n_pair_fields"] and info_s["contract_pair_chunk"] == 0
+        assert mo.rel_l2_per_mode(out_t, out_s).max() < tol
+        assert mo.rel_l2_per_mode(out_t, mo.solve(prob)).max() < (TOL64 if fl else TOL32)
