@@ -948,14 +948,16 @@ std::vector<float> tc_operand(const std::vector<double>& A, int M, int P) {
   return B;
 }
 
-// Build the dense contraction form for this solve? When its term count is above half
-// the dense matrix's size (M^2 P) the register-blocked product does less work than the
-// term loop. MMP_DENSE=0 / 1 forces the choice (M <= 16 either way).
+// Build the dense contraction form for this solve? Per sample, the register-blocked
+// product spends about 36 instructions on every (p, pair field) couple (all kDenseMaxModes
+// k at once), the term loop about 7 on every term, so the dense form pays from 5 M P
+// terms on. MMP_DENSE=0 / 1 forces the choice (M <= 16 either way).
 bool dense_wanted(const mmp_batch* b, const Member& s) {
   (void)b;
   if (s.M > (uint32_t)kDenseMaxModes || s.pairs.empty()) return false;
-  if (const char* env = std::getenv("MMP_DENSE")) return std::atoi(env) == 1;
-  return 2 * s.terms.size() > (size_t)s.M * s.M * s.pairs.size();
+  if (const char* env = std::getenv("MMP_DENSE"))
+    if (*env) return std::atoi(env) == 1;
+  return s.terms.size() > 5 * (size_t)s.M * s.pairs.size();
 }
 
 size_t member_bytes(const mmp_batch* b, const Member& s) {
