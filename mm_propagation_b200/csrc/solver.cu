@@ -167,7 +167,7 @@ int ensure_device(int dev, DeviceRes** out) {
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_pc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 110 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                224 * 1024));
+                                227 * 1024 - 256));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
@@ -1198,6 +1198,7 @@ bool batch_shape(mmp_batch* b) {
   bool fused = iir && TT >= 64 && (int)b->nt >= TT;
   if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
     if (std::atoi(env) == 0) fused = false;
+  if (fused) smem += 2 * (size_t)Pmax * t2;  // the tile's carries (k_contract, raman_mode 2)
   int dense = (span == 0 || TT < 64 || !any_dense) ? 0 : (all_dense ? 1 : 2);
   // FP32 batches whose every solve has the dense form with at least kTcMinModes modes run
   // it on the tensor cores (k_contract_tc, tiles of kTcTile samples) when the pair fields
@@ -1213,7 +1214,7 @@ bool batch_shape(mmp_batch* b) {
     TT = kTcTile;
     fused = b->raman;
     dense = 1;
-    smem = ((size_t)Mmax * TT + (size_t)kTcChunk * TT) * sizeof(float2) +
+    smem = ((size_t)Mmax * TT + (size_t)kTcChunk * TT + (b->raman ? 2 * (size_t)Pmax : 0)) * sizeof(float2) +
            2 * 4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float);  // two operand buffers
   } else if (dense) {
     smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
@@ -1237,7 +1238,7 @@ bool batch_shape(mmp_batch* b) {
     while (tc_tt > 64 && (size_t)Mmax * tc_tt > 2 * kPcItems * 256) tc_tt >>= 1;
     while (tc_tt > (int)b->nt) tc_tt >>= 1;
     const size_t budget = b->fp64 ? 110 * 1024 : 72 * 1024;
-    const size_t fixed = (size_t)Mmax * tc_tt * t2 + max_terms * staged;
+    const size_t fixed = (size_t)Mmax * tc_tt * t2 + max_terms * staged + 2 * (size_t)Pmax * t2;
     if (tc_tt >= 64 && (size_t)Mmax * tc_tt <= 2 * kPcItems * 256 && fixed + 8 * (size_t)tc_tt * t2 <= budget) {
       pchunk = (int)std::min<size_t>((size_t)std::max(Pmax, 1), (budget - fixed) / ((size_t)tc_tt * t2));
       TT = tc_tt;

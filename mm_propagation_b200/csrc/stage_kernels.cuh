@@ -976,6 +976,15 @@ template <typename T> struct TileScan {
 // distinct banks per quarter warp; mask 0 is the plain layout.
 __device__ __forceinline__ int wsw(int h, int mask) { return h ^ ((h >> 3) & mask); }
 
+// The states entering tile `tile` for pair fields 0..P-1 (k_raman_carry's output) into
+// shared memory, [q][Re V, Im V]; published by the caller's next barrier.
+template <typename T>
+__device__ __forceinline__ void stage_tile_carries(c2<T>* sC, const SolveDesc& d, int P, int ntiles, int tile) {
+  const c2<T>* tiles = as_t2<T>(d.raman_tiles);
+  for (int i = threadIdx.x; i < 2 * P; i += blockDim.x)
+    sC[i] = tiles[((size_t)(i >> 1) * ntiles + tile) * 2 + (i & 1)];
+}
+
 // The recurrence through one pair field of a contraction tile, by one warp (TT = 32 c
 // samples, 64 <= TT <= 256): V = U_l conj(U_m) is written coalesced to row (pair positions
 // swizzled by wmask), each lane takes its c samples into registers, the lanes' aggregates
@@ -1224,8 +1233,12 @@ __global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_cont
   const int n_terms = d.term_off[M];
   // pair-field rows: swizzled (wsw) when the recurrence runs here, else plain
   const int wmask = raman == 2 ? max(TT >> 6, 1) - 1 : 0;
+  // raman_mode 2: the states entering this tile per pair field (Re V, Im V), staged while
+  // the tile lands
+  V* sC = sW + (size_t)P * TT;
   // dense form: per warp, two chunks of kDenseChunk coefficient rows (cp.async double buffer)
-  T* sA = reinterpret_cast<T*>(sU + (size_t)(M + P) * TT);
+  T* sA = reinterpret_cast<T*>(sC + (raman == 2 ? 2 * (size_t)P : 0));
+  if (raman == 2) stage_tile_carries<T>(sC, d, P, nt / TT, blockIdx.x);
   const size_t dense_elems = DENSE ? (size_t)(blockDim.x >> 5) * 2 * kDenseChunk * 2 * kDenseMaxModes : 0;
   ST* st = reinterpret_cast<ST*>(sA + dense_elems);
   if (stage_terms) {
@@ -1269,11 +1282,8 @@ __global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_cont
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     TileScan<T> ts;
     ts.init(d, TT >> 5, lane);
-    const int ntiles = nt / TT;
-    const V* tiles = as_t2<T>(d.raman_tiles);
     for (int q = warp; q < P; q += nwarps)
-      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)q * TT, wmask,
-                              tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
+      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)q * TT, wmask, sC + 2 * q, kerr, lane);
   }
   __syncthreads();
   // 2. contraction
@@ -1416,6 +1426,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
   V* sW = sU + (size_t)M * TT;                             // [pc][TT], pair positions swizzled
   ST* st = reinterpret_cast<ST*>(sW + (size_t)pc * TT);   // every term, sorted by (p, pair field)
   const int n_terms = d.term_off[M];
+  V* sC = reinterpret_cast<V*>(st + n_terms);               // states entering the tile, [P][2]
+  stage_tile_carries<T>(sC, d, P, nt / TT, blockIdx.x);
   for (int j = threadIdx.x; j < n_terms; j += blockDim.x) {
     const Term tm = d.terms[j];
     ST x;
@@ -1434,8 +1446,6 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
   const int H = TT >> 1, nitems = M * H;
   const int wmask = max(TT >> 6, 1) - 1;
   const T kerr = (T)d.one_minus_fR;
-  const int ntiles = nt / TT;
-  const V* tiles = as_t2<T>(d.raman_tiles);
   TileScan<T> ts;
   ts.init(d, TT >> 5, lane);
   T acc[kPcItems][4];
@@ -1451,8 +1461,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
   for (int c0 = 0; c0 < P; c0 += pc) {
     const int c1 = min(P, c0 + pc);
     for (int q = c0 + warp; q < c1; q += nwarps)
-      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)(q - c0) * TT, wmask,
-                              tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
+      tile_pair_recurrence<T>(ts, sU, TT, d.pairs[q], sW + (size_t)(q - c0) * TT, wmask, sC + 2 * q, kerr, lane);
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < kPcItems; ++i) {
@@ -1526,6 +1535,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
   V* sW = sU + (size_t)M * TT;                                   // [KC][TT], pair positions swizzled
   float* sA = reinterpret_cast<float*>(sW + (size_t)KC * TT);    // [2][4][KC/4][TT][4]
   float* sB = sA + 2 * 4 * KC * TT;                              // [2][4][KC/4][N][4]
+  V* sC = reinterpret_cast<V*>(sB + 2 * 4 * KC * N);              // states entering the tile, [P][2]
   if (tid == 0) {
     mbar_init(&bar_u, 1);
     for (int i = 0; i < 2; ++i) {
@@ -1540,6 +1550,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
     mbar_wait(&bar_u, 0, kMaxWaitPolls);
     return;
   }
+  if (raman_mode == 2) stage_tile_carries<float>(sC, d, P, nt / TT, blockIdx.x);
   if (warp == 0) {
     tc::alloc(&s_tmem, 512);
     tc::relinquish();
@@ -1550,8 +1561,6 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
   const uint32_t tmem = s_tmem;
   TileScan<float> ts;
   if (raman_mode == 2) ts.init(d, TT >> 5, lane);
-  const int ntiles = nt / TT;
-  const V* tiles = as_t2<float>(d.raman_tiles);
   const float kerr = (float)d.one_minus_fR;
   const int nch = (P + KC - 1) / KC;
   const unsigned bbytes = (unsigned)(4 * KC * N * sizeof(float));
@@ -1575,8 +1584,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
       if (q >= P) continue;
       V* row = sW + (size_t)j * TT;
       if (raman_mode == 2) {
-        tile_pair_recurrence<float>(ts, sU, TT, d.pairs[q], row, WMASK,
-                                    tiles + ((size_t)q * ntiles + blockIdx.x) * 2, kerr, lane);
+        tile_pair_recurrence<float>(ts, sU, TT, d.pairs[q], row, WMASK, sC + 2 * q, kerr, lane);
       } else {
         const int2 lm = d.pairs[q];
         for (int h = lane; h < TT / 2; h += 32) {
