@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     constexpr int NQ = decltype(nqc)::value;
     // frequencies per chunk: all of a chunk's loads are in flight together (8 when the
     // stage reads only psi_hat)
-    constexpr int CHK0 = NQ == 0 ? 8 : 2;
+    constexpr int CHK0 = NQ == 0 ? 8 : 4;
     constexpr int CHK = CHK0 < Gm::E ? CHK0 : Gm::E;
     const double nb3 = d.n_beta == 3;
 #pragma unroll 1
