@@ -121,6 +121,8 @@ struct SolveDesc {
   double2 iir_lambda;
   double2 iir_kappa;
   double2 iir_inv_one_minus;
+  // [kRamanPow] (T complex): lambda^j, j < kRamanPow, computed once in FP64 (iir solves)
+  const void* raman_pow;
   // [P][NT/16][2] (T complex): per contraction tile and pair field, the recurrence's
   // tile aggregate (k_raman_agg), then the state entering the tile (k_raman_carry)
   void* raman_tiles;
@@ -137,6 +139,8 @@ struct SolveDesc {
 // Largest mode count of the dense contraction form (its accumulators live in registers),
 // and the coefficient rows a warp stages in shared memory per chunk.
 constexpr int kDenseMaxModes = 16;
+// Powers of the Raman recurrence's lambda kept per solve (the largest contraction tile).
+constexpr int kRamanPow = 256;
 constexpr int kDenseChunk = 16;
 // Tensor-core form of the dense contraction: samples per tile (the MMA's M), pair fields
 // per K chunk, and the fewest modes a solve needs for it (from 6 modes, 21 pair fields,

@@ -972,6 +972,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + (b->raman ? P : 0) * nt * t2);                           // W (R)
   off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));    // H
   off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);                // Raman tile carries
+  off = align_up(off + (b->raman ? kRamanPow : 0) * t2);                         // powers of lambda
   off = align_up(off + (dense_wanted(b, s) ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));  // dense form
   off = align_up(off + (dense_wanted(b, s) && !b->fp64 ? tc_floats(M, P) * sizeof(float) : 0));  // tensor-core form
   off = align_up(off + s.poly.size() * sizeof(double));
@@ -1033,6 +1034,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_w = off; off = align_up(off + (b->raman ? P : 0) * nt * t2);
   const size_t o_h = off; off = align_up(off + (b->raman ? nt : 0) * std::max(t2, sizeof(double2)));
   const size_t o_rt = off; off = align_up(off + (b->raman ? P * (nt / 16) * 2 : 0) * t2);
+  const size_t o_rp = off; off = align_up(off + (b->raman ? kRamanPow : 0) * t2);
   s.dense_ok = dense_wanted(b, s);
   const size_t o_dq = off; off = align_up(off + (s.dense_ok ? M * P * 2 * kDenseMaxModes * (t2 / 2) : 0));
   const bool tc_ok = s.dense_ok && !b->fp64;
@@ -1074,6 +1076,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.W = T2ptr(s.block, o_w);
   d.H = b->raman ? T2ptr(s.block, o_h) : nullptr;
   d.raman_tiles = b->raman ? T2ptr(s.block, o_rt) : nullptr;
+  d.raman_pow = b->raman ? T2ptr(s.block, o_rp) : nullptr;
   d.dense_q = s.dense_ok ? T2ptr(s.block, o_dq) : nullptr;
   d.dense_tc = tc_ok ? (const float*)T2ptr(s.block, o_tc) : nullptr;
   d.pairs = (const int2*)T2ptr(s.block, o_pairs);
@@ -1097,6 +1100,25 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
       d.iir_lambda = make_double2(lam.real(), lam.imag());
       d.iir_kappa = make_double2(kap.real(), kap.imag());
       d.iir_inv_one_minus = make_double2(inv.real(), inv.imag());
+      // lambda^j, j < kRamanPow, by binary powering in FP64 (the tile aggregates' weights)
+      std::vector<double2> pw64(kRamanPow);
+      std::vector<float2> pw32(kRamanPow);
+      for (int j = 0; j < kRamanPow; ++j) {
+        std::complex<double> r(1.0, 0.0), base = lam;
+        for (int e = j; e; e >>= 1) {
+          if (e & 1) r *= base;
+          base *= base;
+        }
+        pw64[j] = make_double2(r.real(), r.imag());
+        pw32[j] = make_float2((float)r.real(), (float)r.imag());
+      }
+      if (b->fp64)
+        CUDA_TRY(cudaMemcpyAsync((void*)d.raman_pow, pw64.data(), kRamanPow * sizeof(double2), cudaMemcpyHostToDevice,
+                                 b->stream));
+      else
+        CUDA_TRY(cudaMemcpyAsync((void*)d.raman_pow, pw32.data(), kRamanPow * sizeof(float2), cudaMemcpyHostToDevice,
+                                 b->stream));
+      CUDA_TRY(cudaStreamSynchronize(b->stream));  // the tables are host temporaries
     }
   }
   CUDA_TRY(cudaMemcpyAsync((void*)d.poly, s.poly.data(), s.poly.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));

@@ -1051,14 +1051,14 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
   if (t0 >= nt || d.M == 0) return;  // empty slot
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   V* sU = reinterpret_cast<V*>(smem_raw);
-  V* wt = sU + (size_t)d.M * TT;
-  {  // the U tile as 16-byte asynchronous copies, issued before the step check
+  V* sp = sU + (size_t)d.M * TT;  // lambda^j, j < TT
+  {  // the U tile and the powers of lambda as 16-byte asynchronous copies, before the step check
     const V* U = as_t2<T>(d.U);
     const int per_row = TT * (int)sizeof(V) / 16;
-    for (int idx = threadIdx.x; idx < d.M * per_row; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < (d.M + 1) * per_row; idx += blockDim.x) {
       const int r = idx / per_row, c = idx - r * per_row;
-      cp_async16(reinterpret_cast<char*>(sU + (size_t)r * TT) + 16 * c,
-                 reinterpret_cast<const char*>(U + (size_t)r * nt + t0) + 16 * c);
+      const V* src = r < d.M ? U + (size_t)r * nt + t0 : as_t2<T>(d.raman_pow);
+      cp_async16(reinterpret_cast<char*>(sU + (size_t)r * TT) + 16 * c, reinterpret_cast<const char*>(src) + 16 * c);
     }
     cp_async_commit();
   }
@@ -1068,16 +1068,8 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
   }
   // The aggregate over the tile from a zero start is a weighted sum,
   //   S_end = sum_t lambda^(TT-1-t) x_t   (x = Re or Im of U_l conj(U_m)),
-  // so it needs no sequential pass: the weights sit in a table, each lane sums its
-  // samples (32 apart, coalesced) and the warp adds the lanes.
-  for (int t = threadIdx.x; t < TT; t += blockDim.x) {  // lambda^(TT-1-t), FP64 powers
-    double2 r = make_double2(1.0, 0.0), b = d.iir_lambda;
-    for (int e = TT - 1 - t; e; e >>= 1) {
-      if (e & 1) r = cmul(r, b);
-      b = cmul(b, b);
-    }
-    wt[t] = from_d2<T>(r);
-  }
+  // so it needs no sequential pass: each lane sums sample pairs (2h, 2h + 1), h = lane,
+  // lane + 32, ..., weighted from the table of powers, and the warp adds the lanes.
   cp_async_wait<0>();
   __syncthreads();
   const int ntiles = nt / TT;
@@ -1085,11 +1077,14 @@ __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__
   for (int q = warp; q < d.P; q += nwarps) {
     const int2 lm = d.pairs[q];
     V sa = mk<T>(0, 0), sb = mk<T>(0, 0);
-    for (int t = lane; t < TT; t += 32) {
-      const V x = cmulc(sU[lm.x * TT + t], sU[lm.y * TT + t]);
-      const V w = wt[t];
-      sa = mk<T>(fma(w.x, x.x, sa.x), fma(w.y, x.x, sa.y));
-      sb = mk<T>(fma(w.x, x.y, sb.x), fma(w.y, x.y, sb.y));
+    for (int h = lane; h < (TT >> 1); h += 32) {
+      V ul0, ul1, um0, um1, wb, wa;
+      ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
+      ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
+      ld2<T>(sp + TT - 2 - 2 * h, wb, wa);  // lambda^(TT-2-2h) for sample 2h+1, lambda^(TT-1-2h) for 2h
+      const V x0 = cmulc(ul0, um0), x1 = cmulc(ul1, um1);
+      sa = mk<T>(fma(wa.x, x0.x, fma(wb.x, x1.x, sa.x)), fma(wa.y, x0.x, fma(wb.y, x1.x, sa.y)));
+      sb = mk<T>(fma(wa.x, x0.y, fma(wb.x, x1.y, sb.x)), fma(wa.y, x0.y, fma(wb.y, x1.y, sb.y)));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
