@@ -1236,8 +1236,9 @@ bool batch_shape(mmp_batch* b) {
     TT = kTcTile;
     fused = b->raman;
     dense = 1;
-    smem = ((size_t)Mmax * TT + (size_t)kTcChunk * TT + (b->raman ? 2 * (size_t)Pmax : 0)) * sizeof(float2) +
-           2 * 4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float);  // two operand buffers
+    smem = ((size_t)Mmax * TT + (b->raman ? 2 * (size_t)Pmax : 0)) * sizeof(float2) +
+           2 * 4 * (size_t)kTcChunk * (TT + 16 * (size_t)Mmax) * sizeof(float) +  // two operand buffers
+           1024;                                                                  // their alignment
   } else if (dense) {
     smem += 8 * 2 * (size_t)kDenseChunk * 2 * kDenseMaxModes * (t2 / 2);  // staged coefficient rows
   }

@@ -989,25 +989,40 @@ __device__ __forceinline__ void stage_tile_carries(c2<T>* sC, const SolveDesc& d
 // samples, 64 <= TT <= 256): V = U_l conj(U_m) is written coalesced to row (pair positions
 // swizzled by wmask), each lane takes its c samples into registers, the lanes' aggregates
 // are scanned, every lane runs the recurrence from the state entering it (carry[0..1]: the
-// states entering the tile for Re V and Im V) and W = (1 - f_R) V + R goes back in place.
-template <typename T>
-__device__ __forceinline__ void tile_pair_recurrence(const TileScan<T>& ts, const c2<T>* sU, int TT, int2 lm,
-                                                     c2<T>* row, int wmask, const c2<T>* carry, T kerr,
-                                                     int lane) {
+// states entering the tile for Re V and Im V) and hands W = (1 - f_R) V + R for its samples
+// c lane .. c lane + c - 1 to fin(x) (tile_pair_recurrence: back into row, in place). With
+// DIRECT each lane forms V for its own samples straight from U (row unused).
+template <typename T, bool DIRECT = false, typename Fin>
+__device__ __forceinline__ void tile_pair_recurrence_to(const TileScan<T>& ts, const c2<T>* sU, int TT, int2 lm,
+                                                        c2<T>* row, int wmask, const c2<T>* carry, T kerr,
+                                                        int lane, Fin&& fin) {
   using V = c2<T>;
   const int H = TT >> 1, c = ts.c, g = c >> 1;
-  // V = U_l conj(U_m), coalesced over the sample pairs
-  for (int h = lane; h < H; h += 32) {
-    V ul0, ul1, um0, um1;
-    ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
-    ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
-    st2<T>(row + 2 * wsw(h, wmask), cmulc(ul0, um0), cmulc(ul1, um1));
-  }
-  __syncwarp();
   V x[8];
+  if constexpr (!DIRECT) {
+    // V = U_l conj(U_m), coalesced over the sample pairs, then each lane's own samples
+    for (int h = lane; h < H; h += 32) {
+      V ul0, ul1, um0, um1;
+      ld2<T>(sU + lm.x * TT + 2 * h, ul0, ul1);
+      ld2<T>(sU + lm.y * TT + 2 * h, um0, um1);
+      st2<T>(row + 2 * wsw(h, wmask), cmulc(ul0, um0), cmulc(ul1, um1));
+    }
+    __syncwarp();
 #pragma unroll
-  for (int j = 0; j < 4; ++j)
-    if (j < g) ld2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+    for (int j = 0; j < 4; ++j)
+      if (j < g) ld2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j < g) {
+        V ul0, ul1, um0, um1;
+        ld2<T>(sU + lm.x * TT + 2 * (g * lane + j), ul0, ul1);
+        ld2<T>(sU + lm.y * TT + 2 * (g * lane + j), um0, um1);
+        x[2 * j] = cmulc(ul0, um0);
+        x[2 * j + 1] = cmulc(ul1, um1);
+      }
+    }
+  }
   // this lane's aggregate from a zero start: sum_k lambda^(c-1-k) x_k, x_k = Re or Im V
   V la = mk<T>(0, 0), lb = mk<T>(0, 0);
 #pragma unroll
@@ -1037,9 +1052,18 @@ __device__ __forceinline__ void tile_pair_recurrence(const TileScan<T>& ts, cons
                    fma(kerr, x[k].y, fma(ts.kt.x, sb.y, ts.kt.y * sb.x)));
     }
   }
+  fin(x);
+}
+template <typename T>
+__device__ __forceinline__ void tile_pair_recurrence(const TileScan<T>& ts, const c2<T>* sU, int TT, int2 lm,
+                                                     c2<T>* row, int wmask, const c2<T>* carry, T kerr,
+                                                     int lane) {
+  const int g = ts.c >> 1;
+  tile_pair_recurrence_to<T>(ts, sU, TT, lm, row, wmask, carry, kerr, lane, [&](const c2<T>* x) {
 #pragma unroll
-  for (int j = 0; j < 4; ++j)
-    if (j < g) st2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+    for (int j = 0; j < 4; ++j)
+      if (j < g) st2<T>(row + 2 * wsw(g * lane + j, wmask), x[2 * j], x[2 * j + 1]);
+  });
 }
 
 template <typename T>
@@ -1506,18 +1530,23 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
 // fields in chunks of kTcChunk = 16. Both operands are split x = hi + lo into TF32 parts
 // and every product is formed as hi hi + hi lo + lo hi with FP32 accumulation: relative
 // error about 2^-21 (plain TF32 would leave 2^-11).
-// Per chunk c the 16 warps build the chunk's pair fields W in shared memory, one field each
-// (the Raman recurrence through the tile, raman_mode 2, or V = U_l conj(U_m), raman_mode 0),
-// pack them into the MMA's operand layout (buffer c % 2), and one thread issues the chunk's
-// 12 MMAs and commits them to an mbarrier; the chunk's split coefficients
-// (SolveDesc::dense_tc) arrive by one bulk copy issued when the chunk starts. The MMAs of
-// chunk c run while the warps build chunk c + 1. Every wait is bounded: on a timeout the
-// CTA flags kStatusTimeout, waits once more for its MMAs and frees its TMEM.
+// Per chunk c the 16 warps build the chunk's pair fields W, one field each (the Raman
+// recurrence through the tile, raman_mode 2, or V = U_l conj(U_m), raman_mode 0), and each
+// lane writes its 4 consecutive samples, split into TF32 hi and lo, straight into the A
+// operands (buffer c % 2) in the MN-major TF32 layout (samples contiguous: the 4 samples of
+// one field are one 16-byte chunk per matrix); one thread issues the chunk's 12 MMAs and
+// commits them to an mbarrier; the chunk's split coefficients (SolveDesc::dense_tc, K-major)
+// arrive by one bulk copy issued when the chunk starts. The MMAs of chunk c run while the
+// warps build chunk c + 1. Every wait is bounded: on a timeout the CTA flags kStatusTimeout,
+// waits once more for its MMAs and frees its TMEM.
 template <typename T>
 __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restrict__ descs, int nt, int raman_mode) {
   static_assert(sizeof(T) == 4, "TF32 operands come from FP32 solves");
   using V = float2;
   constexpr int TT = kTcTile, KC = kTcChunk, WMASK = TT / 64 - 1;
+  // A operand (MN-major TF32 layout): 32-sample atoms 512 bytes apart, 4-field groups 2048
+  static_assert(TT == 128 && KC % 8 == 0, "one MMA covers the tile's 128 samples");
+  constexpr uint32_t A_LBO = 512, A_SBO = 2048;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bar_u, bar_b[2], bar_m[2];
   __shared__ uint32_t s_tmem;
@@ -1527,8 +1556,10 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
   const int M = d.M, P = d.P, N = 16 * M;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   V* sU = reinterpret_cast<V*>(smem_raw);                        // [M][TT]
-  V* sW = sU + (size_t)M * TT;                                   // [KC][TT], pair positions swizzled
-  float* sA = reinterpret_cast<float*>(sW + (size_t)KC * TT);    // [2][4][KC/4][TT][4]
+  // [2][4][KC * TT] MN-major operands, on the next 1024-byte boundary (the swizzle pattern's
+  // alignment; the launch reserves the slack)
+  unsigned char* after_u = reinterpret_cast<unsigned char*>(sU + (size_t)M * TT);
+  float* sA = reinterpret_cast<float*>(after_u + ((1024u - (tc::smem_u32(after_u) & 1023u)) & 1023u));
   float* sB = sA + 2 * 4 * KC * TT;                              // [2][4][KC/4][N][4]
   V* sC = reinterpret_cast<V*>(sB + 2 * 4 * KC * N);              // states entering the tile, [P][2]
   if (tid == 0) {
@@ -1559,7 +1590,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
   const float kerr = (float)d.one_minus_fR;
   const int nch = (P + KC - 1) / KC;
   const unsigned bbytes = (unsigned)(4 * KC * N * sizeof(float));
-  const uint32_t idesc = tc::idesc_tf32(TT, N);
+  const uint32_t idesc = tc::idesc_tf32(TT, N, true);
   int committed = -1;  // last chunk whose MMAs were committed
   for (int c = 0; c < nch && ok; ++c) {
     const int buf = c & 1;
@@ -1576,45 +1607,37 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
     }
     for (int j = warp; j < KC; j += nwarps) {  // pair field q = c KC + j, one warp each
       const int q = c * KC + j;
-      if (q >= P) continue;
-      V* row = sW + (size_t)j * TT;
-      if (raman_mode == 2) {
-        tile_pair_recurrence<float>(ts, sU, TT, d.pairs[q], row, WMASK, sC + 2 * q, kerr, lane);
+      // lane L's samples 4L .. 4L + 3 of field j: one 16-byte chunk of each operand matrix
+      float* a0 = A + tc::mn_tf32_offset(4 * lane, j, A_LBO, A_SBO) / 4;
+      auto put = [&](const V* x) {
+        float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          rh[e] = tc::tf32_hi(x[e].x);
+          rl[e] = x[e].x - rh[e];
+          ih[e] = tc::tf32_hi(x[e].y);
+          il[e] = x[e].y - ih[e];
+        }
+        *reinterpret_cast<float4*>(a0) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<float4*>(a0 + KC * TT) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+        *reinterpret_cast<float4*>(a0 + 2 * KC * TT) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<float4*>(a0 + 3 * KC * TT) = make_float4(il[0], il[1], il[2], il[3]);
+      };
+      if (q >= P) {  // past the last field: zeros (the buffers start uninitialised)
+        const V z[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        put(z);
+      } else if (raman_mode == 2) {
+        tile_pair_recurrence_to<float, true>(ts, sU, TT, d.pairs[q], nullptr, WMASK, sC + 2 * q, kerr, lane, put);
       } else {
         const int2 lm = d.pairs[q];
-        for (int h = lane; h < TT / 2; h += 32) {
-          V ul0, ul1, um0, um1;
-          ld2<float>(sU + lm.x * TT + 2 * h, ul0, ul1);
-          ld2<float>(sU + lm.y * TT + 2 * h, um0, um1);
-          st2<float>(row + 2 * wsw(h, WMASK), cmulc(ul0, um0), cmulc(ul1, um1));
-        }
-      }
-    }
-    __syncthreads();
-    // pack: sample t, pair fields 4 jq .. 4 jq + 3 of the chunk -> one 16-byte group in
-    // each of the four operand matrices (fields beyond P are zero)
-    for (int it = tid; it < (KC / 4) * TT; it += blockDim.x) {
-      const int jq = it / TT, t = it - jq * TT;
-      const int pos = 2 * wsw(t >> 1, WMASK) + (t & 1);
-      float rh[4], rl[4], ih[4], il[4];
+        V x[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int j = 4 * jq + i;
-        const V w = (c * KC + j < P) ? sW[(size_t)j * TT + pos] : make_float2(0.f, 0.f);
-        rh[i] = tc::tf32_hi(w.x);
-        rl[i] = w.x - rh[i];
-        ih[i] = tc::tf32_hi(w.y);
-        il[i] = w.y - ih[i];
+        for (int e = 0; e < 4; ++e) x[e] = cmulc(sU[lm.x * TT + 4 * lane + e], sU[lm.y * TT + 4 * lane + e]);
+        put(x);
       }
-      float4* a4 = reinterpret_cast<float4*>(A) + (size_t)jq * TT + t;
-      a4[0] = make_float4(rh[0], rh[1], rh[2], rh[3]);
-      a4[KC * TT / 4] = make_float4(rl[0], rl[1], rl[2], rl[3]);
-      a4[2 * KC * TT / 4] = make_float4(ih[0], ih[1], ih[2], ih[3]);
-      a4[3 * KC * TT / 4] = make_float4(il[0], il[1], il[2], il[3]);
     }
     tc::fence_proxy_async();
     // the chunk's coefficients have landed and every thread's operand writes are done
-    // (sW is free again for the next chunk once this barrier is passed)
     ok = __syncthreads_and(mbar_wait(&bar_b[buf], (c >> 1) & 1, kMaxWaitPolls) ? 1 : 0);
     if (!ok) break;
     tc::fence_after_sync();
@@ -1627,9 +1650,9 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
         for (int term = 0; term < 3; ++term)
 #pragma unroll
           for (int ks = 0; ks < KC / 8; ++ks) {
-            const float* a = A + (size_t)(2 * part + ta[term]) * KC * TT + ks * 2 * TT * 4;
+            const float* a = A + (size_t)(2 * part + ta[term]) * KC * TT + ks * 2 * A_SBO / 4;
             const float* b = B + (size_t)(2 * part + tb[term]) * KC * N + ks * 2 * N * 4;
-            tc::mma_tf32(tmem + 256u * part, tc::desc_kmajor(a, TT * 16, 128), tc::desc_kmajor(b, N * 16, 128),
+            tc::mma_tf32(tmem + 256u * part, tc::desc_mn_tf32(a, A_LBO, A_SBO), tc::desc_kmajor(b, N * 16, 128),
                          idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
           }
       tc::commit(&bar_m[buf]);

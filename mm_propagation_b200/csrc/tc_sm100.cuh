@@ -29,10 +29,27 @@ __device__ __forceinline__ uint64_t desc_kmajor(const void* base, uint32_t lbo_b
   return d;
 }
 
+// MN-major TF32 operand (the one swizzled layout the tensor core takes for MN-major 32-bit
+// operands, "128B with 32-byte atoms"): atoms of 4 K-rows x 128 bytes (32 values along M or
+// N), 512-byte aligned, in which the 32-byte chunk index (address bits 5-6) is XORed with
+// the row index (bits 7-8). LBO = bytes between consecutive atoms along M/N, SBO = bytes
+// between consecutive 4-row groups along K; layout type 1 in bits 61-63.
+__device__ __forceinline__ uint64_t desc_mn_tf32(const void* base, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  return desc_kmajor(base, lbo_bytes, sbo_bytes) | ((uint64_t)1 << 61);
+}
+// Byte offset of element (mn, k) in such an operand.
+__host__ __device__ __forceinline__ uint32_t mn_tf32_offset(int mn, int k, uint32_t lbo, uint32_t sbo) {
+  const int r = k & 3, chunk = (mn >> 3) & 3;
+  return (uint32_t)(k >> 2) * sbo + (uint32_t)(mn >> 5) * lbo + (uint32_t)r * 128u +
+         (uint32_t)((chunk ^ r) << 5) + (uint32_t)((mn & 7) << 2);
+}
+
 // Instruction descriptor (32 bits): FP32 accumulator (bits 4-5 = 1), A and B in TF32
-// (bits 7-9 and 10-12 = 2), both K-major (bits 15, 16 = 0), N / 8 at bit 17, M / 16 at bit 24.
-__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// (bits 7-9 and 10-12 = 2), A K-major (bit 15 = 0) or MN-major (1), B K-major (bit 16 = 0),
+// N / 8 at bit 17, M / 16 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool a_mn_major = false) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (a_mn_major ? (1u << 15) : 0u) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
 }
 
 // D[tmem] (+)= A * B^T for one K step of 8; issued by a single thread.
