@@ -297,3 +297,14 @@ def test_raman_recurrence_in_tall_tiles(mmp, monkeypatch):
         assert 0 < info_t["contract_pair_chunk"] < info_t["n_pair_fields"] and info_s["contract_pair_chunk"] == 0
         assert mo.rel_l2_per_mode(out_t, out_s).max() < tol
         assert mo.rel_l2_per_mode(out_t, mo.solve(prob)).max() < (TOL64 if fl else TOL32)
+
+
+def test_dense_contraction_on_tensor_cores_16_modes(mmp, monkeypatch):
+    # the largest tensor-core shape: N = 256 accumulator columns per part (all of TMEM),
+    # 136 pair fields in 9 K chunks (the last one partial)
+    prob = _dense_case(98, 16, 256, 3, True)
+    out_t, info_t = run(mmp, prob, [3])
+    monkeypatch.setenv("MMP_TC", "0")
+    out_s, _ = run(mmp, prob, [3])
+    assert info_t["tensor_core_contraction"] == 1 and info_t["n_pair_fields"] == 136
+    assert mo.rel_l2_per_mode(out_t, out_s).max() < 2e-6
