@@ -603,11 +603,12 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   const bool same_z = zi == znext;
   float p_part_f = 0.0f;
   const float w0f = (float)d.omega0_T0, asf = (float)d.alpha_scale;
-  auto body = [&](auto nqc) {
+  // NQ: the (compile-time) most stored terms the body reads; nqr: how many it reads
+  auto body = [&](auto nqc, int nqr) {
     constexpr int NQ = decltype(nqc)::value;
     // frequencies per chunk: all of a chunk's loads are in flight together (8 when the
     // stage reads only psi_hat)
-    constexpr int CHK0 = NQ == 0 ? 8 : 4;
+    constexpr int CHK0 = NQ == 0 ? 8 : (NQ <= 3 ? 4 : 2);
     constexpr int CHK = CHK0 < Gm::E ? CHK0 : Gm::E;
     const double nb3 = d.n_beta == 3;
 #pragma unroll 1
@@ -623,7 +624,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         ps[c] = d.psi_hat[row + kk[c]];
         sv[c] = s[pad(li)];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) nj[c][q] = Nh[(size_t)s_jq[q] * mstride + row + kk[c]];
+        for (int q = 0; q < NQ; ++q)
+          if (q < nqr) nj[c][q] = Nh[(size_t)s_jq[q] * mstride + row + kk[c]];
       }
 #pragma unroll
       for (int c = 0; c < CHK; ++c) {
@@ -646,9 +648,11 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
           V inc = mk<T>((T)cself * nh.x, (T)cself * nh.y);
 #pragma unroll
           for (int q = 0; q < NQ; ++q) {
-            const T cq = (T)s_cq[q];
-            inc.x = fma(cq, nj[c][q].x, inc.x);
-            inc.y = fma(cq, nj[c][q].y, inc.y);
+            if (q < nqr) {
+              const T cq = (T)s_cq[q];
+              inc.x = fma(cq, nj[c][q].x, inc.x);
+              inc.y = fma(cq, nj[c][q].y, inc.y);
+            }
           }
           const double2 x = make_double2(ps[c].x + (double)inc.x, ps[c].y + (double)inc.y);
           d.psi_hat[row + k] = x;
@@ -669,9 +673,11 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
           x.y = fma(cself, nhd.y, x.y);
 #pragma unroll
           for (int q = 0; q < NQ; ++q) {
-            const double2 v = to_d2(nj[c][q]);
-            x.x = fma(s_cq[q], v.x, x.x);
-            x.y = fma(s_cq[q], v.y, x.y);
+            if (q < nqr) {
+              const double2 v = to_d2(nj[c][q]);
+              x.x = fma(s_cq[q], v.x, x.x);
+              x.y = fma(s_cq[q], v.y, x.y);
+            }
           }
           d.psi_hat[row + k] = x;
           const double a2 = x.x * x.x + x.y * x.y;
@@ -686,9 +692,11 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
           xt.y = fma(cs, nh.y, xt.y);
 #pragma unroll
           for (int q = 0; q < NQ; ++q) {
-            const T cq = (T)s_cq[q];
-            xt.x = fma(cq, nj[c][q].x, xt.x);
-            xt.y = fma(cq, nj[c][q].y, xt.y);
+            if (q < nqr) {
+              const T cq = (T)s_cq[q];
+              xt.x = fma(cq, nj[c][q].x, xt.x);
+              xt.y = fma(cq, nj[c][q].y, xt.y);
+            }
           }
         }
         V en;
@@ -700,11 +708,16 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   };
   // One body per kernel: every extra copy of this loop grows the kernel, and a larger
   // kernel runs its transforms slower (measured: the forward transform ran ~50% slower
-  // with seven copies). Counts other than 0 and 3 take the generic loop.
+  // with seven copies). The generic instantiation (stages of the order-6 and order-8
+  // tableaus) runs the same body with the count at run time (at most kFastQ stored terms,
+  // loads predicated), and an element-wise loop beyond that.
+  constexpr int kFastQ = 5;
   if constexpr (BODY == 0) {
-    body(std::integral_constant<int, 0>{});
+    body(std::integral_constant<int, 0>{}, 0);
   } else if constexpr (BODY == 3) {
-    body(std::integral_constant<int, 3>{});
+    body(std::integral_constant<int, 3>{}, 3);
+  } else if (nq <= kFastQ) {
+    body(std::integral_constant<int, kFastQ>{}, nq);
   } else {
 #pragma unroll 2
   for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
