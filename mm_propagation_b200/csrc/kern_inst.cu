@@ -25,8 +25,18 @@ KernelSet MMP_CAT4(make_kernels_, MMP_TAG, MMP_LOGN, MMP_XC)() {
   k.prime = (const void*)&k_prime<T, L, X>;
   k.pair = (const void*)&k_pair<T, L, X>;
   k.nu = (const void*)&k_nu<T, L, X, -1>;
-  k.nu0 = (const void*)&k_nu<T, L, X, 0>;
-  k.nu3 = (const void*)&k_nu<T, L, X, 3>;
+  // specialised stage bodies: RK4's (0 and last-3) in both precisions, the order-6 and
+  // order-8 tableaus' (intermediate 1..5, last 4) in FP32
+  k.nu_mid[0] = (const void*)&k_nu<T, L, X, 0>;
+  k.nu_last[3] = (const void*)&k_nu<T, L, X, kNuLastBody + 3>;
+  if constexpr (sizeof(T) == 4) {
+    k.nu_mid[1] = (const void*)&k_nu<T, L, X, 1>;
+    k.nu_mid[2] = (const void*)&k_nu<T, L, X, 2>;
+    k.nu_mid[3] = (const void*)&k_nu<T, L, X, 3>;
+    k.nu_mid[4] = (const void*)&k_nu<T, L, X, 4>;
+    k.nu_mid[5] = (const void*)&k_nu<T, L, X, 5>;
+    k.nu_last[4] = (const void*)&k_nu<T, L, X, kNuLastBody + 4>;
+  }
   k.result = (const void*)&k_result<T, L, X>;
   k.dft_fwd = (const void*)&k_dft<T, L, X, false>;
   k.dft_inv = (const void*)&k_dft<T, L, X, true>;

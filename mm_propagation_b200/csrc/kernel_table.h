@@ -7,9 +7,9 @@ namespace mmp {
 struct KernelSet {
   const void* prime = nullptr;
   const void* pair = nullptr;
-  const void* nu = nullptr;   // k_nu for any stage
-  const void* nu0 = nullptr;  // ... for stages with 0 stored N_hat_j terms
-  const void* nu3 = nullptr;  // ... for stages with 3
+  const void* nu = nullptr;          // k_nu for any stage
+  const void* nu_mid[6] = {};        // ... for intermediate stages reading n stored N_hat_j
+  const void* nu_last[5] = {};       // ... for last stages reading n (null: not built)
   const void* result = nullptr;
   const void* dft_fwd = nullptr;
   const void* dft_inv = nullptr;

@@ -153,7 +153,9 @@ int ensure_device(int dev, DeviceRes** out) {
       for (int xc = 0; xc < 2; ++xc) {
         KernelSet ks = kernels_for(fp64, L, xc);
         if (!ks.prime) continue;
-        const void* fns[] = {ks.prime, ks.pair, ks.nu, ks.nu0, ks.nu3, ks.result, ks.dft_fwd, ks.dft_inv};
+        std::vector<const void*> fns = {ks.prime, ks.pair, ks.nu, ks.result, ks.dft_fwd, ks.dft_inv};
+        for (const void* f : ks.nu_mid) if (f) fns.push_back(f);
+        for (const void* f : ks.nu_last) if (f) fns.push_back(f);
         for (const void* f : fns)
           CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
       }
@@ -603,9 +605,9 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
   return MMP_OK;
 }
 
-// The k_nu instantiation for stage i: an intermediate stage with no stored N_hat_j
-// terms, or a last stage with 3 (the counts k_nu's thread 0 derives), takes its
-// specialised body; every other stage the generic one.
+// The k_nu instantiation for stage i: a stage whose count of stored N_hat_j terms (the
+// count k_nu's thread 0 derives) has a specialised body built takes it; every other
+// stage the generic one.
 const void* nu_kernel(const KernelSet& ks, const Tableau& tab, int i) {
   const bool last = i == tab.s - 1;
   int nq = 0;
@@ -614,8 +616,8 @@ const void* nu_kernel(const KernelSet& ks, const Tableau& tab, int i) {
   } else {
     for (int j = 0; j < i; ++j) nq += (tab.a[i + 1][j] != 0.0);
   }
-  if (nq == 0 && !last) return ks.nu0;
-  if (nq == 3 && last) return ks.nu3;
+  if (!last && nq < 6 && ks.nu_mid[nq]) return ks.nu_mid[nq];
+  if (last && nq < 5 && ks.nu_last[nq]) return ks.nu_last[nq];
   return ks.nu;
 }
 

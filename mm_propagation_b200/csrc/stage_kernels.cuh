@@ -491,10 +491,11 @@ __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict_
 }
 
 // ---- k_nu: sigma_p -> N_hat_i, final accumulation, next stage's U ------------------------
-// BODY: the stage arithmetic of an intermediate stage with no stored N_hat_j terms (0),
-// of a last stage with 3 (3), or of any stage (-1). The host launches the instantiation
-// that matches each stage of its tableau (RK4: 0 at the intermediate stages, 3 at the
-// last), so each kernel carries one body.
+// BODY: the stage arithmetic of an intermediate stage that reads n stored N_hat_j terms
+// (BODY = n), of a last stage that reads n (BODY = kNuLastBody + n), or of any stage (-1).
+// The host launches the instantiation that matches each stage of its tableau (RK4: 0 at
+// the intermediate stages, kNuLastBody + 3 at the last), so each kernel carries one body.
+constexpr int kNuLastBody = 10;
 template <typename T, int LOGN, int XC, int BODY>
 __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_BLOCKS) k_nu(const KParams kp) {
   using Gm = Geo<T, LOGN, XC>;
@@ -580,9 +581,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers publish them and the values thread 0 wrote
   const int i = kp.stage;
   const int S = kp.tab.s;
-  // BODY 0 serves intermediate stages only and BODY 3 last stages only: fixed at compile
-  // time, so each instantiation carries only its half of the stage arithmetic
-  const bool last = BODY < 0 ? (i == S - 1) : (BODY == 3);
+  // a specialised BODY serves intermediate or last stages only: fixed at compile time, so
+  // each instantiation carries only its half of the stage arithmetic
+  const bool last = BODY < 0 ? (i == S - 1) : (BODY >= kNuLastBody);
   const double h = d.dz;
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
@@ -712,10 +713,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // tableaus) runs the same body with the count at run time (at most kFastQ stored terms,
   // loads predicated), and an element-wise loop beyond that.
   constexpr int kFastQ = 5;
-  if constexpr (BODY == 0) {
-    body(std::integral_constant<int, 0>{}, 0);
-  } else if constexpr (BODY == 3) {
-    body(std::integral_constant<int, 3>{}, 3);
+  if constexpr (BODY >= 0) {
+    constexpr int NQB = BODY >= kNuLastBody ? BODY - kNuLastBody : BODY;
+    body(std::integral_constant<int, NQB>{}, NQB);
   } else if (nq <= kFastQ) {
     body(std::integral_constant<int, kFastQ>{}, nq);
   } else {
