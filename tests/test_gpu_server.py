@@ -60,6 +60,25 @@ def test_requests_joining_a_running_pool(mmp):
         assert np.array_equal(out, single(mmp, p))
 
 
+def test_dense_requests_on_the_tensor_cores_in_a_pool(mmp):
+    # dense-Q requests (M >= 6, FP32): the pool's contraction runs on the tensor cores for
+    # all of them, as each does alone; they finish at different steps while the pool runs
+    probs = []
+    for i, (m, n) in enumerate([(6, 7), (7, 4), (6, 10)]):
+        p = W.dense15(seed=300 + i, M=m, nt=256, n_steps=n, raman=True)
+        probs.append(W.scale_power(p, W.phase_cap_scale(p, per_step=0.05, total=0.3)))
+    with mmp.Server(max_slots=4, steps_per_tick=2) as sv:
+        ids = [sv.submit(p) for p in probs]
+        outs = [sv.wait(i, timeout=120) for i in ids]
+    for p, (out, info) in zip(probs, outs):
+        assert info["status"] == 0 and info["steps"] == p.n_steps
+        with mmp.Solver(p) as s:
+            s.propagate(p.n_steps)
+            alone, sinfo = s.result(), s.info()
+        assert sinfo["tensor_core_contraction"] == 1
+        assert np.array_equal(out, alone)
+
+
 def test_memory_budget_serialises_and_rejects(mmp):
     small = [W.small_case(seed=260 + i, M=2, nt=512, n_steps=6) for i in range(3)]
     with mmp.Server(memory_budget=200 * 1024, steps_per_tick=3) as sv:
