@@ -8,18 +8,24 @@
 // one inverse transform per mode to get U and one forward transform per mode
 // to turn sigma into N_hat, instead of two of each.
 //
-// One RK stage i of step n is three launches (two with Raman off):
-//   k_pair      per pair field (l<=m):  V = U_l conj(U_m) -> FFT -> * H_R -> IFFT = R
-//                                                                       (Raman on only)
-//   k_contract  per time tile:          sigma_p = sum Q U_k [(1-fR) U_l conj(U_m) + R_lm]
-//                                       (all p; Raman off: sum Q U_k U_l conj(U_m))
-//   k_nu        per mode p:             FFT(sigma_p) -> N_hat_i = i sgn(gamma) conj(E_i) *.,
-//                                       [last stage: psi_hat += h sum b_j N_hat_j, monitors],
-//                                       x_hat = psi_hat + h sum a_{i+1,j} N_hat_j,
-//                                       * E_{i+1} -> IFFT -> U for the next stage
-// k_prime makes U for stage 0 when a propagate call starts. E_i = exp(i Im L_p(w) z)
-// is never stored: the phase Im L_p(w) * (z_n + c_i h) is evaluated in FP64,
-// reduced mod 2 pi in FP64 and only then passed to sincos in T.
+// One RK stage i of step n is, with Raman on and h_R a damped sinusoid (every workload),
+// four launches; two with Raman off:
+//   k_raman_agg    per time tile:   the Raman recurrence's aggregate over the tile for
+//                                   every pair field V = U_l conj(U_m)
+//   k_raman_carry  per pair field:  tile aggregates -> the state entering each tile
+//   k_contract     per time tile:   R through the tile from that state, then
+//                                   sigma_p = sum Q U_k [(1-fR) V_lm + R_lm] (all p)
+//                  (k_contract_pc for tiles with too many pair fields to hold at once,
+//                   k_contract_tc for dense Q on the tensor cores)
+//   k_nu           per mode p:      FFT(sigma_p) -> N_hat_i = i sgn(gamma) conj(E_i) *.,
+//                                   [last stage: psi_hat += h sum b_j N_hat_j, monitors],
+//                                   x_hat = psi_hat + h sum a_{i+1,j} N_hat_j,
+//                                   * E_{i+1} -> IFFT -> U for the next stage
+// Any other h_R takes k_pair (V -> FFT -> * H_R -> IFFT = R per pair field) instead of
+// the first two, and k_contract reads R as rows. k_prime makes U for stage 0 when a
+// propagate call starts. E_i = exp(i Im L_p(w) z) is never stored: the phase
+// Im L_p(w) * (z_n + c_i h) is evaluated in FP64, reduced in FP64 and only then passed
+// to sin/cos in T.
 #pragma once
 
 #include <type_traits>
