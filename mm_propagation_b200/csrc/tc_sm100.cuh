@@ -2,12 +2,13 @@
 // memory (TMEM) allocation, shared-memory matrix descriptors, the TF32 MMA with FP32
 // accumulators in TMEM, its completion on an mbarrier, and TMEM loads.
 //
-// Operand layout used throughout (K-major, no swizzle): a matrix of R rows by K 32-bit
-// values is stored as [K/4][R][4], i.e. for every group of 4 consecutive K values the R
-// rows follow each other 16 bytes apart. The hardware's 8-row x 16-byte core matrices are
-// then contiguous 128-byte blocks (stride-byte offset SBO = 128 between 8-row groups) and
-// the two 16-byte K halves of one MMA (K = 8 for TF32) are R * 16 bytes apart (leading-byte
-// offset LBO). The MMA's K step advances the start address by 2 * R * 16 bytes.
+// Two operand layouts are described here. K-major without swizzle (desc_kmajor): a matrix
+// of R rows by K 32-bit values stored as [K/4][R][4], i.e. for every group of 4 consecutive
+// K values the R rows follow each other 16 bytes apart; the hardware's 8-row x 16-byte core
+// matrices are then contiguous 128-byte blocks (stride-byte offset SBO = 128 between 8-row
+// groups) and the two 16-byte K halves of one MMA (K = 8 for TF32) are R * 16 bytes apart
+// (leading-byte offset LBO), so the MMA's K step advances the start address by 2 R 16 bytes.
+// MN-major TF32 (desc_mn_tf32, mn_tf32_offset): see below.
 #pragma once
 
 #include <cuda_runtime.h>
