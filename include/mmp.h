@@ -37,6 +37,7 @@ extern "C" {
 #define MMP_ENOTSUP (-6)    /* valid input outside what this build supports (e.g. NT not 2^k) */
 #define MMP_ENODEV (-7)     /* no usable sm_100 device */
 #define MMP_ESTATE (-8)     /* call not valid in the object's current state */
+#define MMP_EDRIFT (-9)     /* the FP64 energy left the band set by mmp_set_energy_drift_limit */
 
 /* ---- flags (mmp_params.flags) ---------------------------------------------------- */
 /* Arithmetic: default is FP32 bulk (FFTs, contraction, Raman) with FP64 dispersion
@@ -115,6 +116,14 @@ typedef struct mmp_info {
                                                (tcgen05, TF32 operands split hi + lo, FP32 sums) */
   uint32_t contract_pair_chunk;             /* > 0: pair fields held per chunk by the contraction
                                                of tall tiles (Raman recurrence in the tiles) */
+  uint32_t contract_sub_block;              /* > 0: the contraction of tall tiles runs the Raman
+                                               recurrence serially per pair field, in sub-blocks of
+                                               this many samples (merged terms) */
+  uint32_t contract_tile;                   /* samples per contraction tile (CTA) */
+  uint32_t autotuned;                       /* 1: cluster_ctas, contract_tile and graph_branches
+                                               were chosen by timing steps of this batch on
+                                               this device (or taken from that choice, cached
+                                               for the same shape) */
 } mmp_info;
 
 typedef struct mmp_solver mmp_solver;
@@ -163,6 +172,16 @@ int mmp_get_monitors(mmp_solver* s, double* energy, double* photons, uint64_t ma
 
 int mmp_get_info(mmp_solver* s, mmp_info* info);
 
+/* No counterpart in the reference, which checks nothing while it propagates. Failure
+ * detection from the FP64 energy monitor: after every step the device compares the
+ * step's total energy E with E_ref, the energy after the first step since creation or
+ * mmp_set_fields, and flags the solve when |E - E_ref| > rel_tol * E_ref; the next
+ * mmp_propagate / mmp_synchronize returns MMP_EDRIFT. rel_tol = 0 turns the check off
+ * (the default). Energy is a conserved quantity of the Kerr system with a coupling
+ * symmetric in (p, k, l, m); with Raman on it is not exactly conserved, so choose the
+ * band accordingly. MMP_ESTATE if the solve keeps no monitors (MMP_F_NO_MONITORS). */
+int mmp_set_energy_drift_limit(mmp_solver* s, double rel_tol);
+
 /* ~MultimodePropagation (include/MultimodePropagation.hpp:39). NULL is allowed. */
 void mmp_solver_destroy(mmp_solver* s);
 
@@ -209,6 +228,8 @@ int mmp_batch_get_result(mmp_batch* b, uint32_t index, double* out);
 int mmp_batch_set_fields(mmp_batch* b, uint32_t index, const double* phi0);
 int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info);
 uint32_t mmp_batch_size(const mmp_batch* b);
+/* mmp_set_energy_drift_limit for member `index`. */
+int mmp_batch_set_energy_drift_limit(mmp_batch* b, uint32_t index, double rel_tol);
 void mmp_batch_destroy(mmp_batch* b);
 
 /* ---- serving: a request loop with continuous batching ---------------------------------
@@ -294,6 +315,19 @@ const char* mmp_last_error(void);
 const char* mmp_version(void);
 /* Number of this library's kernels launched so far in this process (all devices). */
 uint64_t mmp_kernel_launch_count(void);
+
+/* ---- test hooks (no counterpart in the reference) -------------------------------------
+ * Allocation-failure injection: after `after` more successful device allocations by
+ * this library, the next one fails as if the device were out of memory (the call that
+ * made it returns MMP_ENOMEM); after < 0 turns injection off. One-shot. */
+int mmp_debug_fail_alloc(int64_t after);
+/* Device allocations this library holds (made and not yet freed), all devices: for
+ * checking that a failed call leaks nothing. Includes one twiddle table per device.
+ * The environment variable MMP_TILE_WAIT_POLLS, read when a solve is created, sets how
+ * many polls the contraction kernels give the first wait for their tile copy (default
+ * 2^24, far above any copy time); 0 makes that bounded wait give up at once, so the
+ * propagate call reports MMP_ETIMEOUT (the copies still land before a CTA leaves). */
+int64_t mmp_debug_live_allocations(void);
 
 #ifdef __cplusplus
 }

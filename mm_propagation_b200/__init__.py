@@ -126,6 +126,11 @@ class Solver:
         _check(lib().mmp_get_info(self._ptr, C.byref(i)), "mmp_get_info")
         return info_dict(i)
 
+    def set_energy_drift_limit(self, rel_tol: float):
+        """Fail later propagate calls with MMP_EDRIFT once the FP64 energy monitor moves by
+        more than rel_tol of the first step's energy (0 turns the check off)."""
+        _check(lib().mmp_set_energy_drift_limit(self._ptr, float(rel_tol)), "mmp_set_energy_drift_limit")
+
     def close(self):
         if self._ptr:
             lib().mmp_solver_destroy(self._ptr)
@@ -197,6 +202,10 @@ class Batch:
         inf = capi.mmp_info()
         _check(lib().mmp_batch_get_info(self._ptr, i, C.byref(inf)), "mmp_batch_get_info")
         return info_dict(inf)
+
+    def set_energy_drift_limit(self, i: int, rel_tol: float):
+        _check(lib().mmp_batch_set_energy_drift_limit(self._ptr, i, float(rel_tol)),
+               "mmp_batch_set_energy_drift_limit")
 
     def close(self):
         if self._ptr:

@@ -31,7 +31,7 @@ CXX = os.environ.get("MMP_CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++")
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I", INCLUDE]
 LOGN_RANGE = range(6, 17)
 # row-split variants (kernel_table.h kSplit*): log2 NT ranges per precision
-SPLIT_F32 = range(12, 16)
+SPLIT_F32 = range(12, 17)
 SPLIT_F64 = range(11, 15)
 
 

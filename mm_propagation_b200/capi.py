@@ -22,6 +22,7 @@ MMP_ETIMEOUT = -5
 MMP_ENOTSUP = -6
 MMP_ENODEV = -7
 MMP_ESTATE = -8
+MMP_EDRIFT = -9
 
 MMP_F_FP64 = 1 << 0
 MMP_F_PHYSICAL_PAIRS = 1 << 1
@@ -79,6 +80,9 @@ class mmp_info(C.Structure):
         ("dense_contraction", C.c_uint32),
         ("tensor_core_contraction", C.c_uint32),
         ("contract_pair_chunk", C.c_uint32),
+        ("contract_sub_block", C.c_uint32),
+        ("contract_tile", C.c_uint32),
+        ("autotuned", C.c_uint32),
     ]
 
 
@@ -148,6 +152,10 @@ SIGNATURES = {
     "mmp_last_error": (C.c_char_p, []),
     "mmp_version": (C.c_char_p, []),
     "mmp_kernel_launch_count": (C.c_uint64, []),
+    "mmp_set_energy_drift_limit": (C.c_int, [C.c_void_p, C.c_double]),
+    "mmp_batch_set_energy_drift_limit": (C.c_int, [C.c_void_p, C.c_uint32, C.c_double]),
+    "mmp_debug_fail_alloc": (C.c_int, [C.c_int64]),
+    "mmp_debug_live_allocations": (C.c_int64, []),
 }
 
 _lib = None

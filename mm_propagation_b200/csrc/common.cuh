@@ -54,6 +54,7 @@ __host__ __device__ constexpr int padded_len(int n) { return n + (n >> 5); }
 // SolveDesc::status bits
 constexpr int kStatusNonFinite = 1;  // the field became NaN/Inf
 constexpr int kStatusTimeout = 2;    // a bounded device-side wait gave up
+constexpr int kStatusDrift = 4;      // the FP64 energy left the band set by drift_tol
 
 // Maximum number of RK stages (Butcher11) and dispersion orders handled.
 constexpr int kMaxStages = 11;
@@ -107,9 +108,12 @@ struct SolveDesc {
   double* energy;             // [mon_cap]
   double* photons;            // [mon_cap]
   unsigned long long mon_cap;
-  int* status;                // bit 0: non-finite field seen
+  int* status;                // kStatus* bits
   int monitors;               // 1: accumulate monitors
-  int pad_;
+  // Polls the contraction kernels give the first wait for their tile copy before they
+  // report kStatusTimeout (they then still wait, with the full bound, for the copy to
+  // land before leaving). The host sets it far above any copy time.
+  unsigned tile_wait_polls;
   // Stage kernels do nothing for this solve once *step >= step_limit (a solve in a
   // served pool stops at its own step count while the pool's graph keeps running).
   unsigned long long step_limit;
@@ -134,6 +138,22 @@ struct SolveDesc {
   // fields, four K-major matrices [Re hi, Re lo, Im hi, Im lo][kTcChunk/4][16 M][4] of
   // TF32 values (x = hi + lo), row (p, k) = 16 p + k; null if unused
   const float* dense_tc;
+  // Energy drift check (0 = off): the last CTA of each step's final stage compares the
+  // step's FP64 energy with *drift_ref (the first step's energy after creation or
+  // set_fields) and sets kStatusDrift when |E - E_ref| > drift_tol E_ref.
+  double drift_tol;
+  double* drift_ref;
+  // The contraction's terms merged per (p, k, pair field q) for k_contract_sr: a term
+  // reading W_q and one reading conj(W_q) with the same k add up to
+  //   U_k (a Re W_q + i b Im W_q),  a = Q1 + Q2, b = Q1 - Q2,
+  // sorted by p (sr_off[p] .. sr_off[p + 1]); sr_coef holds (a, a, b, b) in FP32 solves and
+  // (a, b) in FP64 ones, sr_kq = k | q << 16, sr_perm the modes by descending term count.
+  const void* sr_coef;
+  const unsigned* sr_kq;
+  const int* sr_off;   // [M + 1]
+  const int* sr_perm;  // [M]
+  int sr_terms;
+  int pad3_;
 };
 
 // Largest mode count of the dense contraction form (its accumulators live in registers),

@@ -25,7 +25,7 @@ constexpr int kMinLogN = 6;
 constexpr int kMaxLogN = 16;
 
 // Row-split variants built besides xc = 0 (FP32 / FP64 ranges of log2 NT).
-constexpr int kSplitMinLogN32 = 12, kSplitMaxLogN32 = 15;
+constexpr int kSplitMinLogN32 = 12, kSplitMaxLogN32 = 16;
 constexpr int kSplitMinLogN64 = 11, kSplitMaxLogN64 = 14;
 
 // Defined in the kern_inst.cu objects; returns an empty set for variants not built.

@@ -26,6 +26,10 @@
 // data in it. Nothing in it needs to start at zero (each call writes every sample
 // it reads), but calls that overlap on the GPU — from several host threads — race
 // on it; serialise them.
+//
+// Errors are reported like every other entry point's: a negative MMP_E* code, and
+// the text in mmp_last_error() on the calling thread (recorded into a fixed buffer,
+// without allocating). Its kernel launches are counted in mmp_kernel_launch_count().
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -71,11 +75,16 @@ std::mutex g_mu;
 constexpr int kMaxDevices = 64;
 NoallocDevice g_devs[kMaxDevices];  // fixed table: no allocation on any call
 
-thread_local char g_err[256];
-int fail(int code, const char* msg) {
-  std::snprintf(g_err, sizeof(g_err), "%s", msg);
-  return code;
-}
+}  // namespace
+
+namespace mmp_detail {
+int set_error_c(int code, const char* msg);  // solver.cu: the text mmp_last_error returns
+void count_launch();                          // solver.cu: mmp_kernel_launch_count
+}  // namespace mmp_detail
+
+namespace {
+
+int fail(int code, const char* msg) { return mmp_detail::set_error_c(code, msg); }
 
 int setup(int dev, NoallocDevice** out) {
   if (dev < 0 || dev >= kMaxDevices) return fail(MMP_ENODEV, "device ordinal out of range");
@@ -93,6 +102,7 @@ int setup(int dev, NoallocDevice** out) {
   float2* f = reinterpret_cast<float2*>(r.base + kTwD);
   k_fill_twiddles<<<256, 256>>>(d, f);
   e = cudaGetLastError();
+  if (e == cudaSuccess) mmp_detail::count_launch();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(MMP_ECUDA, cudaGetErrorString(e));
   for (int L = 0; L <= kMaxLogN; ++L) {
@@ -158,6 +168,7 @@ int mmp_dft_noalloc(uint32_t n, uint32_t rows, int direction, int fp64, const do
       cfg.numAttrs = 1;
     }
     e = cudaLaunchKernelExC(&cfg, direction < 0 ? ks.dft_fwd : ks.dft_inv, args);
+    if (e == cudaSuccess) mmp_detail::count_launch();
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, stage, bytes, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(MMP_ECUDA, cudaGetErrorString(e));

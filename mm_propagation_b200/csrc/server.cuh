@@ -35,6 +35,7 @@ struct Request {
   std::vector<mmp_nz> nz;
   // outcome
   int status = MMP_OK;
+  std::string error;  // the failure's text, recorded on the worker thread
   bool done = false;
   uint64_t steps = 0;
   double t_submit = 0, t_start = -1, t_done = -1;
@@ -71,6 +72,7 @@ struct mmp_server {
   uint64_t used_bytes = 0;
   std::chrono::steady_clock::time_point t0;
   int fatal = MMP_OK;  // a CUDA error the worker could not recover from
+  std::string fatal_msg;  // its text (the worker's own last-error is thread-local)
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
@@ -121,8 +123,8 @@ size_t footprint(const mmp_params* p) {
 void clear_slot(Pool& pl, uint32_t slot) {
   mmp_batch* b = pl.b;
   Member& s = b->members[slot];
-  if (s.block) cudaFreeAsync(s.block, b->stream);
-  if (s.energy) cudaFree(s.energy);
+  dev_free(s.block, b->stream, true);
+  dev_free(s.energy);
   s = Member();
   b->active[slot] = 0;
   upload_desc(b);
@@ -156,11 +158,23 @@ int admit(mmp_server* sv, Request* r, int pi, uint32_t slot) {
   return MMP_OK;
 }
 
-void finish(mmp_server* sv, Request* r, int status, std::vector<double>* result) {
+// The worker thread's failures are recorded in its own thread-local last-error; the
+// text travels with the request (and the fatal error with the server) so that the
+// client thread's mmp_server_wait can report it through mmp_last_error.
+void set_fatal(mmp_server* sv, int rc) {
+  if (rc == MMP_OK || sv->fatal != MMP_OK) return;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->fatal = rc;
+  sv->fatal_msg = g_last_error;
+}
+
+void finish(mmp_server* sv, Request* r, int status, std::vector<double>* result, const char* msg = nullptr) {
   std::lock_guard<std::mutex> lk(sv->mu);
   if (result) r->result.swap(*result);
   r->steps = r->steps_run;
   r->status = status;
+  if (status) r->error = msg ? msg : (sv->fatal == status && !sv->fatal_msg.empty() ? sv->fatal_msg.c_str()
+                                                                                     : g_last_error);
   r->done = true;
   r->t_done = sv->now();
   sv->cv_done.notify_all();
@@ -177,13 +191,23 @@ void complete(mmp_server* sv, int pi, int K) {
     if (r->steps_run < r->p.n_steps && sv->fatal == MMP_OK) continue;
     const Member& s = pl.b->members[slot];
     int status = sv->fatal;
+    const char* msg = nullptr;
     if (status == MMP_OK) {
       int st = 0;
       cudaError_t e = cudaMemcpy(&st, (char*)s.counters + 3 * sizeof(unsigned long long), sizeof(int),
                                  cudaMemcpyDeviceToHost);
-      if (e != cudaSuccess) status = fail(MMP_ECUDA, cudaGetErrorString(e));
-      else if (st & kStatusTimeout) status = MMP_ETIMEOUT;
-      else if (st & kStatusNonFinite) status = MMP_ENONFINITE;
+      if (e != cudaSuccess) {
+        status = fail(MMP_ECUDA, cudaGetErrorString(e));
+      } else if (st & kStatusTimeout) {
+        status = MMP_ETIMEOUT;
+        msg = "a device-side bounded wait gave up";
+      } else if (st & kStatusNonFinite) {
+        status = MMP_ENONFINITE;
+        msg = "non-finite field values (the solve diverged or its input was not finite)";
+      } else if (st & kStatusDrift) {
+        status = MMP_EDRIFT;
+        msg = "the FP64 energy monitor left the band set by the drift limit";
+      }
     }
     std::vector<double> out((size_t)2 * r->p.n_modes * r->p.nt);
     if (status == MMP_OK) status = member_result(pl.b, slot, out.data());
@@ -191,7 +215,7 @@ void complete(mmp_server* sv, int pi, int K) {
     pl.slot_req[slot] = nullptr;
     pl.used -= 1;
     sv->used_bytes -= r->bytes;
-    finish(sv, r, status, status == MMP_OK ? &out : nullptr);
+    finish(sv, r, status, status == MMP_OK ? &out : nullptr, msg);
   }
 }
 
@@ -256,7 +280,7 @@ void worker_loop(mmp_server* sv) {
         any_in_flight = true;
         continue;
       }
-      if (e != cudaSuccess && sv->fatal == MMP_OK) sv->fatal = fail(MMP_ECUDA, cudaGetErrorString(e));
+      if (e != cudaSuccess) set_fatal(sv, fail(MMP_ECUDA, cudaGetErrorString(e)));
       complete(sv, (int)pi, K);
       progressed = true;
     }
@@ -283,7 +307,7 @@ void worker_loop(mmp_server* sv) {
         if (e != cudaSuccess) rc = fail(MMP_ECUDA, cudaGetErrorString(e));
         else g_launches.fetch_add((uint64_t)K * b->kernels_per_step, std::memory_order_relaxed);
       }
-      if (rc && sv->fatal == MMP_OK) sv->fatal = rc;
+      set_fatal(sv, rc);
       if (rc) cudaEventRecord(pl.done_ev, b->stream);  // completes at once; solves fail there
       pl.in_flight = true;
       any_in_flight = true;
@@ -394,8 +418,9 @@ int mmp_server_wait(mmp_server* sv, uint64_t id, double timeout_s, double* out, 
   }
   const int status = r->status;
   if (out && status == MMP_OK) std::memcpy(out, r->result.data(), r->result.size() * sizeof(double));
+  const std::string why = status ? "request failed: " + r->error : std::string();
   sv->requests.erase(it);
-  if (status) return fail(status, "request failed");
+  if (status) return fail(status, why);
   return MMP_OK;
 }
 

@@ -33,7 +33,7 @@ using namespace mmp;
 namespace mmp {
 MMP_DECL_ALL(f32)
 MMP_DECL_ALL(f64)
-MMP_DECL(f32, 12, 1) MMP_DECL(f32, 13, 1) MMP_DECL(f32, 14, 1) MMP_DECL(f32, 15, 1)
+MMP_DECL(f32, 12, 1) MMP_DECL(f32, 13, 1) MMP_DECL(f32, 14, 1) MMP_DECL(f32, 15, 1) MMP_DECL(f32, 16, 1)
 MMP_DECL(f64, 11, 1) MMP_DECL(f64, 12, 1) MMP_DECL(f64, 13, 1) MMP_DECL(f64, 14, 1)
 
 KernelSet kernels_for(int fp64, int logn, int xc) {
@@ -46,7 +46,7 @@ KernelSet kernels_for(int fp64, int logn, int xc) {
       }
     }
     switch (logn) {
-      MMP_CASE(f32, 12, 1) MMP_CASE(f32, 13, 1) MMP_CASE(f32, 14, 1) MMP_CASE(f32, 15, 1)
+      MMP_CASE(f32, 12, 1) MMP_CASE(f32, 13, 1) MMP_CASE(f32, 14, 1) MMP_CASE(f32, 15, 1) MMP_CASE(f32, 16, 1)
       default: return KernelSet();
     }
   }
@@ -72,18 +72,24 @@ KernelSet kernels_for(int fp64, int logn, int xc) {
 namespace {
 
 std::atomic<uint64_t> g_launches{0};
-thread_local std::string g_last_error;
+// Text of the calling thread's last failure (mmp_last_error). A fixed buffer, so that
+// recording a failure never allocates (mmp_dft_noalloc reports through it too).
+thread_local char g_last_error[512];
 
-int fail(int code, const std::string& msg) {
-  g_last_error = msg;
+int fail_c(int code, const char* msg) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg ? msg : "");
   return code;
 }
+int fail(int code, const std::string& msg) { return fail_c(code, msg.c_str()); }
 
 }  // namespace
 
 namespace mmp_detail {
-// for the host-only units (io.cpp): record the text mmp_last_error returns
+// for the other units (io.cpp, noalloc.cu): record the text mmp_last_error returns
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
+int set_error_c(int code, const char* msg) { return fail_c(code, msg); }
+// a kernel launched outside launch() (noalloc.cu), counted in mmp_kernel_launch_count
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace mmp_detail
 
 namespace {
@@ -96,6 +102,33 @@ namespace {
                   std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
     }                                                                                    \
   } while (0)
+
+// ---- device allocations: every one goes through dev_malloc / dev_free ------------------
+// Failure injection for tests (mmp_debug_fail_alloc): after `g_fail_after` more
+// successful allocations the next one fails as cudaErrorMemoryAllocation (-1: never).
+// g_live counts the allocations not yet freed (mmp_debug_live_allocations).
+std::atomic<int64_t> g_fail_after{-1};
+std::atomic<int64_t> g_live{0};
+
+cudaError_t dev_malloc(void** p, size_t bytes, cudaMemPool_t pool = nullptr, cudaStream_t st = nullptr) {
+  int64_t n = g_fail_after.load();
+  while (n >= 0 && !g_fail_after.compare_exchange_weak(n, n - 1)) {
+  }
+  if (n == 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  const cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMalloc(p, bytes);
+  if (e == cudaSuccess) g_live.fetch_add(1);
+  else *p = nullptr;
+  return e;
+}
+void dev_free(void* p, cudaStream_t st = nullptr, bool pooled = false) {
+  if (!p) return;
+  if (pooled) cudaFreeAsync(p, st);
+  else cudaFree(p);
+  g_live.fetch_sub(1);
+}
 
 // shared memory of k_raman_scan: a 128 KB segment of V, padded
 constexpr int kScanSmem = padded_len(128 * 1024 / 8) * 8;
@@ -137,11 +170,15 @@ int ensure_device(int dev, DeviceRes** out) {
     off += n;
   }
   void* mem = nullptr;
-  CUDA_TRY(cudaMalloc(&mem, n_tot * (sizeof(double2) + sizeof(float2))));
+  CUDA_TRY(dev_malloc(&mem, n_tot * (sizeof(double2) + sizeof(float2))));
   double2* dd = (double2*)mem;
   float2* df = (float2*)(dd + n_tot);
-  CUDA_TRY(cudaMemcpy(dd, hd.data(), n_tot * sizeof(double2), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(df, hf.data(), n_tot * sizeof(float2), cudaMemcpyHostToDevice));
+  cudaError_t ce = cudaMemcpy(dd, hd.data(), n_tot * sizeof(double2), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(df, hf.data(), n_tot * sizeof(float2), cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) {
+    dev_free(mem);
+    return fail(MMP_ECUDA, std::string("twiddle upload: ") + cudaGetErrorString(ce));
+  }
   for (int L = 0; L <= kMaxLogN; ++L) {
     r.tw.d[L] = L ? dd + offs[L] : nullptr;
     r.tw.f[L] = L ? df + offs[L] : nullptr;
@@ -170,6 +207,10 @@ int ensure_device(int dev, DeviceRes** out) {
                                 110 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 227 * 1024 - 256));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_sr<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)&k_contract_sr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<float>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kScanSmem));
   CUDA_TRY(cudaFuncSetAttribute((const void*)&k_raman_scan<double>,
@@ -302,6 +343,11 @@ struct Member {
   std::vector<int2> pairs;
   std::vector<Term> terms;
   std::vector<int> term_off;
+  // terms merged per (p, k, pair field) for k_contract_sr: coefficients (a, b), k | q << 16,
+  // offsets per p, modes by descending merged-term count
+  std::vector<double> sr_ab;
+  std::vector<unsigned> sr_kq;
+  std::vector<int> sr_off, sr_perm;
   std::vector<double> poly;
   bool quirk = false;
   bool dense_ok = false;  // the dense contraction form is built for this solve
@@ -462,6 +508,32 @@ void host_setup(const mmp_params* p, Member& s) {
                      [](const Term& a, const Term& b) { return (a.pc & 0x7fff) < (b.pc & 0x7fff); });
   }
   s.term_off[M] = (int)s.terms.size();
+  // merged terms: Q1 W + Q2 conj(W) = (Q1 + Q2) Re W + i (Q1 - Q2) Im W for the terms of p
+  // with the same k and pair field (both readings of a symmetric coupling), one record each
+  s.sr_ab.clear();
+  s.sr_kq.clear();
+  s.sr_off.assign(M + 1, 0);
+  for (uint32_t q = 0; q < M; ++q) {
+    s.sr_off[q] = (int)s.sr_kq.size();
+    std::map<std::pair<int, int>, std::pair<double, double>> merged;  // (pair, k) -> (a, b)
+    for (int j = s.term_off[q]; j < s.term_off[q + 1]; ++j) {
+      const Term& t = s.terms[j];
+      auto& ab = merged[std::make_pair((int)(t.pc & 0x7fff), (int)t.k)];
+      ab.first += t.q;
+      ab.second += (t.pc & 0x8000) ? -t.q : t.q;
+    }
+    for (const auto& e : merged) {
+      s.sr_ab.push_back(e.second.first);
+      s.sr_ab.push_back(e.second.second);
+      s.sr_kq.push_back((unsigned)e.first.second | ((unsigned)e.first.first << 16));
+    }
+  }
+  s.sr_off[M] = (int)s.sr_kq.size();
+  s.sr_perm.resize(M);
+  for (uint32_t q = 0; q < M; ++q) s.sr_perm[q] = (int)q;
+  std::stable_sort(s.sr_perm.begin(), s.sr_perm.end(), [&](int x, int y) {
+    return s.sr_off[x + 1] - s.sr_off[x] > s.sr_off[y + 1] - s.sr_off[y];
+  });
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -494,6 +566,9 @@ struct mmp_batch {
   int dense = 0;  // contraction form: 0 term loop, 1 dense (k_contract<T, 1>), 2 per solve
   bool tc = false;  // dense form on the tensor cores (k_contract_tc)
   int pchunk = 0;   // > 0: pair fields per chunk of the pair-chunked contraction (k_contract_pc)
+  bool sr = false;  // serial-recurrence contraction in sub-blocks (k_contract_sr)
+  int tile_req = 0;  // contraction tile asked for by the autotuner (0: batch_shape's own)
+  int tuned = 0;     // 1: launch parameters chosen by timing (autotune)
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> branch_ev;
   cudaEvent_t fork_ev = nullptr;
@@ -536,15 +611,20 @@ int grow_monitors(mmp_batch* b, Member& s, unsigned long long need) {
   unsigned long long cap = std::max<unsigned long long>(need, s.mon_cap * 2);
   cap = std::max<unsigned long long>(cap, 1024);
   double* mem = nullptr;
-  CUDA_TRY(cudaMalloc(&mem, 2 * cap * sizeof(double)));
-  CUDA_TRY(cudaMemsetAsync(mem, 0, 2 * cap * sizeof(double), b->stream));
+  CUDA_TRY(dev_malloc((void**)&mem, 2 * cap * sizeof(double)));
+  cudaError_t e = cudaMemsetAsync(mem, 0, 2 * cap * sizeof(double), b->stream);
   if (s.mon_cap) {
-    CUDA_TRY(cudaMemcpyAsync(mem, s.energy, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
-    CUDA_TRY(cudaMemcpyAsync(mem + cap, s.photons, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice,
-                             b->stream));
-    CUDA_TRY(cudaStreamSynchronize(b->stream));
-    CUDA_TRY(cudaFree(s.energy));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(mem, s.energy, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(mem + cap, s.photons, s.mon_cap * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) {
+    dev_free(mem);
+    return fail(MMP_ECUDA, std::string("monitor buffers: ") + cudaGetErrorString(e));
+  }
+  dev_free(s.energy);
   s.energy = mem;
   s.photons = mem + cap;
   s.mon_cap = cap;
@@ -588,6 +668,13 @@ int launch_contract(mmp_batch* b, uint32_t first = 0, uint32_t count = ~0u, cuda
                        (const void*)&k_contract<float, 2>};
   const void* f64[] = {(const void*)&k_contract<double, 0>, (const void*)&k_contract<double, 1>,
                        (const void*)&k_contract<double, 2>};
+  if (b->sr) {
+    int tb = b->TT;
+    void* sargs[] = {(void*)&descs, &nt, &tb, &mode};
+    const void* fsr = b->fp64 ? (const void*)&k_contract_sr<double> : (const void*)&k_contract_sr<float>;
+    CUDA_TRY(launch(fsr, grid, kSrThreads, (int)b->contract_smem, 1, st ? st : b->stream, sargs));
+    return MMP_OK;
+  }
   if (b->pchunk) {
     int pc = b->pchunk;
     void* pargs[] = {(void*)&descs, &nt, &TT, &pc};
@@ -650,66 +737,6 @@ int launch_pairs(mmp_batch* b, const KernelSet& ks, int nsolves, int stage, cons
   void* args[] = {(void*)&dd, &nt, &seg};
   const void* fn = b->fp64 ? (const void*)&k_raman_scan<double> : (const void*)&k_raman_scan<float>;
   CUDA_TRY(launch(fn, dim3((unsigned)b->Pmax, (unsigned)nsolves, 1), thr, smem, 1, st ? st : b->stream, args));
-  return MMP_OK;
-}
-
-// ---- autotuner: rows on one CTA (or the minimal cluster) vs split over twice as many
-// CTAs. Both variants' pair and per-mode kernels are timed on this batch's own buffers
-// at stage 0 (which rewrites only W, U and N_hat_0: all of them are recomputed before
-// they are read again), and the faster set is kept. Decisions are cached per shape.
-std::mutex g_tune_mu;
-std::map<std::vector<int>, int> g_tune_cache;
-
-int time_variant(mmp_batch* b, const KernelSet& ks, float* ms) {
-  const int nsol = (int)b->span;
-  cudaEvent_t e0, e1;
-  CUDA_TRY(cudaEventCreate(&e0));
-  CUDA_TRY(cudaEventCreate(&e1));
-  int rc = MMP_OK;
-  for (int rep = 0; rep < 4 && rc == MMP_OK; ++rep) {  // rep 0 warms up
-    if (rep == 1) cudaEventRecord(e0, b->stream);
-    rc = launch_pairs(b, ks, nsol, 0, b->d_descs);
-    if (rc == MMP_OK) rc = launch_row_kernel(b, ks, nu_kernel(ks, b->tab, 0), b->Mmax, nsol, 0, b->d_descs);
-  }
-  cudaEventRecord(e1, b->stream);
-  cudaError_t e = cudaEventSynchronize(e1);
-  float f = 0.f;
-  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (rc) return rc;
-  if (e != cudaSuccess) return fail(MMP_ECUDA, cudaGetErrorString(e));
-  *ms = f;
-  return MMP_OK;
-}
-
-int autotune(mmp_batch* b) {
-  const KernelSet alt = kernels_for(b->fp64 ? 1 : 0, b->logn, 1);
-  if (!alt.prime) return MMP_OK;
-  if (const char* env = std::getenv("MMP_ROW_SPLIT")) {  // 0 / 1 forces a variant
-    if (std::atoi(env) == 1) b->ks = alt;
-    return MMP_OK;
-  }
-  const std::vector<int> key = {b->device, b->fp64 ? 1 : 0, b->logn, b->Mmax, b->Pmax,
-                                (int)b->members.size(), b->raman ? 1 : 0};
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_cache.find(key);
-    if (it != g_tune_cache.end()) {
-      if (it->second == 1) b->ks = alt;
-      return MMP_OK;
-    }
-  }
-  const uint64_t counted = g_launches.load();
-  float t0 = 0.f, t1 = 0.f;
-  int rc = time_variant(b, b->ks, &t0);
-  if (rc == MMP_OK) rc = time_variant(b, alt, &t1);
-  g_launches.store(counted);  // tuning launches are not solver work
-  if (rc) return rc;
-  const int pick = (t1 < t0) ? 1 : 0;
-  if (pick) b->ks = alt;
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = pick;
   return MMP_OK;
 }
 
@@ -798,6 +825,8 @@ int check_status(mmp_batch* b) {
   }
   if (bad & kStatusTimeout) return fail(MMP_ETIMEOUT, "a device-side bounded wait gave up");
   if (bad & kStatusNonFinite) return fail(MMP_ENONFINITE, "the field became NaN/Inf during propagation");
+  if (bad & kStatusDrift)
+    return fail(MMP_EDRIFT, "the FP64 energy monitor left the band set by mmp_set_energy_drift_limit");
   return MMP_OK;
 }
 
@@ -882,6 +911,8 @@ int member_set_fields(mmp_batch* b, uint32_t idx, const double* phi0) {
                   b->ks64.C, b->stream, args));
   CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), b->stream));  // z = 0
   CUDA_TRY(cudaMemsetAsync((char*)s.counters + 3 * sizeof(unsigned long long), 0, sizeof(int), b->stream));
+  // the drift check's reference energy: the first step's energy from these fields on
+  CUDA_TRY(cudaMemsetAsync((char*)s.counters + 4 * sizeof(unsigned long long), 0, sizeof(double), b->stream));
   s.step_host = 0;
   return MMP_OK;
 }
@@ -905,7 +936,7 @@ int batch_open(mmp_batch* b, const mmp_params* p0, const Tableau& tab0) {
   if (!b->ks.prime || !b->ks64.prime) return fail(MMP_ENOTSUP, "no kernels built for this nt");
   b->kernels_per_step = b->tab.s * ((b->raman ? 1 : 0) + 2);
   CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  CUDA_TRY(cudaMalloc(&b->d_descs, (size_t)b->capacity * sizeof(SolveDesc)));
+  CUDA_TRY(dev_malloc((void**)&b->d_descs, (size_t)b->capacity * sizeof(SolveDesc)));
   return MMP_OK;
 }
 
@@ -962,6 +993,18 @@ bool dense_wanted(const mmp_batch* b, const Member& s) {
   return s.terms.size() > 5 * (size_t)s.M * s.pairs.size();
 }
 
+// step, total, done counter | status, drift reference energy, spare
+constexpr int kCounterWords = 6;
+
+// Polls the contraction kernels give the first wait for their tile copy: far above any
+// copy time. MMP_TILE_WAIT_POLLS (read when a solve is created) lowers it, for tests that
+// make that bounded wait run out and check that the call reports MMP_ETIMEOUT.
+unsigned tile_wait_polls() {
+  if (const char* env = std::getenv("MMP_TILE_WAIT_POLLS"))
+    if (*env) return (unsigned)std::strtoul(env, nullptr, 10);
+  return kMaxWaitPolls;
+}
+
 size_t member_bytes(const mmp_batch* b, const Member& s) {
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
@@ -981,7 +1024,10 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
   off = align_up(off + (M + 1) * sizeof(int));
-  off = align_up(off + 4 * sizeof(unsigned long long));
+  off = align_up(off + std::max<size_t>(s.sr_kq.size(), 1) * 16);                // merged coefficients
+  off = align_up(off + std::max<size_t>(s.sr_kq.size(), 1) * sizeof(unsigned));  // their k | q << 16
+  off = align_up(off + (2 * M + 1) * sizeof(int));                               // offsets, mode order
+  off = align_up(off + kCounterWords * sizeof(unsigned long long));
   return off;
 }
 
@@ -1045,9 +1091,12 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t o_pairs = off; off = align_up(off + std::max<size_t>(P, 1) * sizeof(int2));
   const size_t o_terms = off; off = align_up(off + std::max<size_t>(s.terms.size(), 1) * sizeof(Term));
   const size_t o_toff = off; off = align_up(off + (M + 1) * sizeof(int));
-  const size_t o_cnt = off; off = align_up(off + 4 * sizeof(unsigned long long));
-  cudaError_t e = b->mempool ? cudaMallocFromPoolAsync(&s.block, off, b->mempool, b->stream)
-                             : cudaMalloc(&s.block, off);
+  const size_t nsr = s.sr_kq.size();
+  const size_t o_src = off; off = align_up(off + std::max<size_t>(nsr, 1) * 16);
+  const size_t o_skq = off; off = align_up(off + std::max<size_t>(nsr, 1) * sizeof(unsigned));
+  const size_t o_soff = off; off = align_up(off + (2 * M + 1) * sizeof(int));
+  const size_t o_cnt = off; off = align_up(off + kCounterWords * sizeof(unsigned long long));
+  cudaError_t e = dev_malloc(&s.block, off, b->mempool, b->stream);
   if (e != cudaSuccess) {
     s.block = nullptr;
     return fail(MMP_ENOMEM, "allocating solver state: " + std::string(cudaGetErrorString(e)));
@@ -1084,13 +1133,21 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.pairs = (const int2*)T2ptr(s.block, o_pairs);
   d.terms = (const Term*)T2ptr(s.block, o_terms);
   d.term_off = (const int*)T2ptr(s.block, o_toff);
+  d.sr_coef = T2ptr(s.block, o_src);
+  d.sr_kq = (const unsigned*)T2ptr(s.block, o_skq);
+  d.sr_off = (const int*)T2ptr(s.block, o_soff);
+  d.sr_perm = d.sr_off + (M + 1);
+  d.sr_terms = (int)nsr;
   s.counters = (unsigned long long*)T2ptr(s.block, o_cnt);
   d.step = s.counters;
   d.total = s.counters + 1;
   d.done_ctr = (unsigned int*)(s.counters + 2);
   d.status = (int*)(s.counters + 3);
+  d.drift_ref = (double*)(s.counters + 4);
+  d.drift_tol = 0.0;
   d.monitors = (s.flags & MMP_F_NO_MONITORS) ? 0 : 1;
   d.step_limit = ~0ull;
+  d.tile_wait_polls = tile_wait_polls();
   if (b->raman) {
     std::complex<double> lam, c;
     if (fit_damped_sinusoid(p->raman_response, (uint32_t)nt, lam, c)) {
@@ -1128,6 +1185,28 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   if (!s.terms.empty())
     CUDA_TRY(cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  {
+    // merged terms (k_contract_sr): FP32 records (a, a, b, b), FP64 records (a, b)
+    std::vector<float> cf32;
+    if (!b->fp64) {
+      cf32.resize(4 * nsr);
+      for (size_t i = 0; i < nsr; ++i) {
+        cf32[4 * i] = cf32[4 * i + 1] = (float)s.sr_ab[2 * i];
+        cf32[4 * i + 2] = cf32[4 * i + 3] = (float)s.sr_ab[2 * i + 1];
+      }
+    }
+    std::vector<int> offs(s.sr_off);
+    offs.insert(offs.end(), s.sr_perm.begin(), s.sr_perm.end());
+    if (nsr) {
+      CUDA_TRY(cudaMemcpyAsync((void*)d.sr_coef, b->fp64 ? (const void*)s.sr_ab.data() : (const void*)cf32.data(),
+                               nsr * 16, cudaMemcpyHostToDevice, b->stream));
+      CUDA_TRY(cudaMemcpyAsync((void*)d.sr_kq, s.sr_kq.data(), nsr * sizeof(unsigned), cudaMemcpyHostToDevice,
+                               b->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync((void*)d.sr_off, offs.data(), offs.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));  // the staging vectors are host temporaries
+  }
   if (s.dense_ok) {
     // A[p][q][k] += Q, A[p][q][16 + k] += Q or -Q (terms that read conj of pair field q)
     constexpr int K = kDenseMaxModes;
@@ -1190,7 +1269,7 @@ bool batch_shape(mmp_batch* b) {
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   int Mmax = 0, Pmax = 0, Pall = 0;
   uint32_t span = 0;
-  size_t max_terms = 0;
+  size_t max_terms = 0, max_sr_terms = 0;
   bool iir = b->raman;
   bool all_dense = true, any_dense = false;
   int Mmin = 1 << 30;
@@ -1206,6 +1285,7 @@ bool batch_shape(mmp_batch* b) {
     Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
     Pall = std::max(Pall, (int)s.pairs.size());
     max_terms = std::max(max_terms, s.terms.size());
+    max_sr_terms = std::max(max_sr_terms, s.sr_kq.size());
   }
   // contraction tile: the largest power of two <= 256 whose U + pair-field tile fits in
   // 100 KB (the pair fields are formed in the tile with Raman on and off)
@@ -1214,6 +1294,7 @@ bool batch_shape(mmp_batch* b) {
   while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
   while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
   while (TT > (int)b->nt) TT >>= 1;
+  if (b->tile_req >= 64 && b->tile_req < TT) TT = b->tile_req;  // a smaller tile the autotuner times
   size_t smem = (size_t)rows * TT * t2;
   if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
     if (std::atoi(env) == 1) iir = false;
@@ -1271,14 +1352,41 @@ bool batch_shape(mmp_batch* b) {
       smem = fixed + (size_t)pchunk * tc_tt * t2;
     }
   }
-  const int stage_terms = pchunk ? 1 : (dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0);
+  // Tall tiles with every pair field formed in the contraction (Raman off, or the
+  // recurrence fused): the serial-recurrence contraction in sub-blocks of kSrSub samples
+  // (k_contract_sr, tiles of up to 256 samples) when its shared memory fits, in place of the
+  // pair-chunked one. MMP_CONTRACT_SR=0 keeps the latter.
+  bool sr = false;
+  {
+    const bool tall = (size_t)rows * 64 * t2 > 100 * 1024;
+    bool ok = tall && span > 0 && !any_dense && Mmax <= kSrMaxModes &&
+              Pall <= kSrPairsPerThread * kSrThreads && (!b->raman || iir) && (int)b->nt >= kSrSub * 4;
+    if (const char* env = std::getenv("MMP_CONTRACT_SR"))
+      if (std::atoi(env) == 0) ok = false;
+    if (const char* env = std::getenv("MMP_RAMAN_FUSED"))
+      if (std::atoi(env) == 0 && b->raman) ok = false;
+    const size_t sp = 2 * t2;  // one sample pair of one row
+    const size_t rs = kSrSub / 2 + 1;
+    const size_t need = (2 * (size_t)Mmax + (size_t)Pall) * rs * sp + max_sr_terms * (16 + sizeof(unsigned)) +
+                        (2 * (size_t)Mmax + 1) * sizeof(int);
+    if (ok && need <= 227 * 1024) {
+      sr = true;
+      pchunk = 0;
+      TT = std::min(b->tile_req >= 64 ? std::min(b->tile_req, 256) : 256, (int)b->nt);
+      fused = b->raman;
+      smem = (need + 15) & ~(size_t)15;
+    }
+  }
+  const int stage_terms = sr ? 0 : (pchunk ? 1 : (dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0));
   if (stage_terms && !pchunk) smem += max_terms * staged;
   const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
                        stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
-                       fused != b->raman_fused || dense != b->dense || tc != b->tc || pchunk != b->pchunk;
+                       fused != b->raman_fused || dense != b->dense || tc != b->tc || pchunk != b->pchunk ||
+                       sr != b->sr;
   b->dense = dense;
   b->tc = tc;
   b->pchunk = pchunk;
+  b->sr = sr;
   b->raman_iir = iir;
   b->raman_fused = fused;
   b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
@@ -1294,6 +1402,150 @@ bool batch_shape(mmp_batch* b) {
     b->graph_steps = 0;
   }
   return changed;
+}
+
+// ---- autotuner -------------------------------------------------------------------------
+// Three launch parameters are chosen by timing whole RK steps of this batch on its own
+// buffers, one parameter after the other (each timed with the others at their current
+// choice):
+//   1. the per-mode transform kernels: each row on the minimal set of CTAs, or split over
+//      twice as many (a cluster twice as wide: one more radix-2 exchange across CTAs and
+//      half the shared memory per CTA, so two CTAs share an SM), where that set is built;
+//   2. the contraction tile: samples per CTA of k_contract (64 / 128 / 256, as many as fit
+//      its shared memory) or of k_contract_sr (64 / 128 / 256);
+//   3. the graph branches: the batch's solves split into 1, 2 or 4 independent kernel
+//      chains per captured step.
+// The timed steps advance the solves; afterwards every member gets its initial fields
+// back at z = 0 with its counters cleared, as if nothing had run. The choice is cached
+// per shape (device, precision, NT, tableau size, largest M and P, batch size, Raman,
+// contraction form). MMP_ROW_SPLIT, MMP_CONTRACT_TILE and MMP_GROUPS each fix one
+// parameter instead.
+struct TuneChoice {
+  int xc = 0, tile = 0, groups = 1;
+};
+std::mutex g_tune_mu;
+std::map<std::vector<int>, TuneChoice> g_tune_cache;
+
+// Device time per RK step of `reps` steps after one warm-up step.
+int time_steps(mmp_batch* b, int reps, float* ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_TRY(cudaEventCreate(&e0));
+  cudaError_t e = cudaEventCreate(&e1);
+  int rc = e == cudaSuccess ? capture_steps(b, 1) : fail(MMP_ECUDA, cudaGetErrorString(e));
+  if (rc == MMP_OK) {
+    cudaEventRecord(e0, b->stream);
+    rc = capture_steps(b, reps);
+    cudaEventRecord(e1, b->stream);
+  }
+  float f = 0.f;
+  if (rc == MMP_OK) {
+    e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+    if (e != cudaSuccess) rc = fail(MMP_ECUDA, cudaGetErrorString(e));
+  } else {
+    cudaStreamSynchronize(b->stream);
+  }
+  cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  *ms = f / (float)reps;
+  return rc;
+}
+
+// Contraction tiles worth timing for the form batch_shape chose (first: its own choice).
+std::vector<int> tile_candidates(const mmp_batch* b) {
+  std::vector<int> t = {b->TT};
+  if (b->tc || b->pchunk) return t;  // fixed tiles
+  if (b->sr || b->TT >= 64)
+    for (int c = 256; c >= 64; c >>= 1)
+      if (c != b->TT && c <= (b->sr ? 256 : b->TT) && c <= (int)b->nt) t.push_back(c);
+  return t;
+}
+
+int restore_members(mmp_batch* b, const mmp_params* const* params) {
+  for (uint32_t i = 0; i < b->members.size(); ++i) {
+    if (!b->active[i]) continue;
+    int rc = member_set_fields(b, i, params[i]->initial_fields);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(b->members[i].counters, 0, kCounterWords * sizeof(unsigned long long), b->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return MMP_OK;
+}
+
+int autotune(mmp_batch* b, const mmp_params* const* params) {
+  const KernelSet base = kernels_for(b->fp64 ? 1 : 0, b->logn, 0);
+  const KernelSet alt = kernels_for(b->fp64 ? 1 : 0, b->logn, 1);
+  std::vector<int> xcs = {0}, tiles = tile_candidates(b), gs = {1};
+  if (alt.prime) xcs.push_back(1);
+  const int g0 = b->span >= 16 ? 4 : (b->span >= 4 ? 2 : 1);  // the untuned default
+  gs = {g0};
+  for (int g : {1, 2, 4})
+    if (g != g0 && (uint32_t)g <= b->span) gs.push_back(g);
+  if (const char* env = std::getenv("MMP_ROW_SPLIT"))
+    if (*env) xcs = {std::atoi(env) == 1 && alt.prime ? 1 : 0};
+  if (const char* env = std::getenv("MMP_CONTRACT_TILE"))
+    if (*env) tiles = {std::atoi(env)};
+  if (const char* env = std::getenv("MMP_GROUPS"))
+    if (*env) gs = {std::max(1, std::atoi(env))};
+  auto apply = [&](const TuneChoice& c) {
+    b->ks = c.xc ? alt : base;
+    b->tile_req = c.tile;
+    batch_shape(b);
+    b->groups = (uint32_t)c.groups;
+  };
+  TuneChoice c;
+  c.xc = xcs[0];
+  c.tile = tiles[0];
+  c.groups = gs[0];
+  b->tuned = 0;
+  if (xcs.size() == 1 && tiles.size() == 1 && gs.size() == 1) {
+    apply(c);
+    return MMP_OK;
+  }
+  const std::vector<int> key = {b->device, b->fp64 ? 1 : 0, b->logn, b->tab.s, b->Mmax, b->Pmax,
+                                (int)b->span, b->raman ? 1 : 0, b->tc ? 1 : 0, b->sr ? 1 : 0,
+                                b->pchunk ? 1 : 0, b->dense, (int)xcs.size(), (int)tiles.size(), (int)gs.size()};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      apply(it->second);
+      b->tuned = 1;
+      return MMP_OK;
+    }
+  }
+  const uint64_t counted = g_launches.load();
+  int rc = MMP_OK;
+  auto sweep = [&](int TuneChoice::*field, const std::vector<int>& vals) {
+    if (vals.size() < 2 || rc) return;
+    float best = 0.f;
+    int pick = c.*field;
+    for (size_t i = 0; i < vals.size() && rc == MMP_OK; ++i) {
+      TuneChoice t = c;
+      t.*field = vals[i];
+      apply(t);
+      float ms = 0.f;
+      rc = time_steps(b, 3, &ms);
+      if (rc == MMP_OK && (i == 0 || ms < best)) {
+        best = ms;
+        pick = vals[i];
+      }
+    }
+    c.*field = pick;
+  };
+  apply(c);
+  sweep(&TuneChoice::xc, xcs);
+  sweep(&TuneChoice::tile, tiles);
+  sweep(&TuneChoice::groups, gs);
+  g_launches.store(counted);  // tuning launches are not solver work
+  if (rc) return rc;
+  apply(c);
+  rc = restore_members(b, params);
+  if (rc) return rc;
+  b->tuned = 1;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = c;
+  return MMP_OK;
 }
 
 int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
@@ -1318,10 +1570,7 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
   for (uint32_t i = 0; i < n && rc == MMP_OK; ++i) rc = member_init(b, i, params[i]);
   if (rc == MMP_OK) {
     batch_shape(b);
-    rc = autotune(b);
-    // graph branches: measured on the 6-mode batch of 32, 2 branches +20%, 4 branches +22%
-    b->groups = b->span >= 16 ? 4 : (b->span >= 4 ? 2 : 1);
-    if (const char* env = std::getenv("MMP_GROUPS")) b->groups = (uint32_t)std::max(1, std::atoi(env));
+    rc = autotune(b, params);
   }
   if (rc == MMP_OK) {
     cudaError_t e = cudaStreamSynchronize(b->stream);
@@ -1360,6 +1609,9 @@ void fill_info(mmp_batch* b, const Member& s, mmp_info* info) {
   info->dense_contraction = (b->dense == 1 || (b->dense == 2 && s.dense_ok)) ? 1u : 0u;
   info->tensor_core_contraction = b->tc ? 1u : 0u;
   info->contract_pair_chunk = (uint32_t)b->pchunk;
+  info->contract_sub_block = b->sr ? (uint32_t)kSrSub : 0u;
+  info->contract_tile = (uint32_t)b->TT;
+  info->autotuned = (uint32_t)b->tuned;
 }
 
 }  // namespace
@@ -1374,7 +1626,7 @@ int mmp_validate_params(const mmp_params* params, char* msg, size_t msg_len) {
   if (msg && msg_len) {
     std::snprintf(msg, msg_len, "%s", rc ? why.c_str() : "");
   }
-  if (rc) g_last_error = why;
+  if (rc) fail(rc, why);
   return rc;
 }
 
@@ -1410,6 +1662,18 @@ int mmp_batch_get_info(mmp_batch* b, uint32_t index, mmp_info* info) {
 }
 
 uint32_t mmp_batch_size(const mmp_batch* b) { return b ? (uint32_t)b->members.size() : 0u; }
+
+int mmp_batch_set_energy_drift_limit(mmp_batch* b, uint32_t index, double rel_tol) {
+  if (!b || index >= b->members.size() || !b->active[index]) return fail(MMP_EINVAL, "bad drift-limit arguments");
+  if (!(rel_tol >= 0.0) || !std::isfinite(rel_tol)) return fail(MMP_EINVAL, "drift limit must be finite and >= 0");
+  Member& s = b->members[index];
+  if (rel_tol > 0.0 && (s.flags & MMP_F_NO_MONITORS))
+    return fail(MMP_ESTATE, "the drift check reads the energy monitor, which MMP_F_NO_MONITORS turns off");
+  CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));  // no launch in flight reads the old descriptor
+  s.desc.drift_tol = rel_tol;
+  return upload_desc(b);
+}
 
 int mmp_batch_propagate_timed(mmp_batch* b, uint32_t nz, uint32_t repeats, double* ms) {
   if (!b || !ms) return fail(MMP_EINVAL, "bad timed-propagate arguments");
@@ -1490,14 +1754,14 @@ void mmp_batch_destroy(mmp_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (auto& s : b->members) {
-    if (s.block) b->mempool ? cudaFreeAsync(s.block, b->stream) : cudaFree(s.block);
-    if (s.energy) cudaFree(s.energy);
+    dev_free(s.block, b->stream, b->mempool != nullptr);
+    dev_free(s.energy);
   }
   if (b->mempool && b->stream) cudaStreamSynchronize(b->stream);
   for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
   for (cudaEvent_t e : b->branch_ev) cudaEventDestroy(e);
   if (b->fork_ev) cudaEventDestroy(b->fork_ev);
-  if (b->d_descs) cudaFree(b->d_descs);
+  dev_free(b->d_descs);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -1595,6 +1859,11 @@ int mmp_get_monitors(mmp_solver* s, double* energy, double* photons, uint64_t ma
   return MMP_OK;
 }
 
+int mmp_set_energy_drift_limit(mmp_solver* s, double rel_tol) {
+  if (!s) return fail(MMP_EINVAL, "NULL solver");
+  return mmp_batch_set_energy_drift_limit(s->b, 0, rel_tol);
+}
+
 int mmp_get_info(mmp_solver* s, mmp_info* info) {
   if (!s || !info) return fail(MMP_EINVAL, "bad info arguments");
   fill_info(s->b, s->b->members[0], info);
@@ -1645,8 +1914,8 @@ int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in
   double2* d_out = nullptr;
   cudaStream_t st = nullptr;
   CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  cudaError_t e = cudaMalloc(&d_in, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&d_out, bytes);
+  cudaError_t e = dev_malloc((void**)&d_in, bytes);
+  if (e == cudaSuccess) e = dev_malloc((void**)&d_out, bytes);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_in, in, bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
     DftArgs a;
@@ -1662,10 +1931,11 @@ int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(d_in);
-  cudaFree(d_out);
+  dev_free(d_in);
+  dev_free(d_out);
   cudaStreamDestroy(st);
-  if (e != cudaSuccess) return fail(MMP_ECUDA, std::string("mmp_dft: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? MMP_ENOMEM : MMP_ECUDA, std::string("mmp_dft: ") + cudaGetErrorString(e));
   return MMP_OK;
 }
 
@@ -1680,15 +1950,23 @@ const char* mmp_strerror(int code) {
     case MMP_ENOTSUP: return "not supported by this build";
     case MMP_ENODEV: return "no sm_100 device";
     case MMP_ESTATE: return "invalid state for this call";
+    case MMP_EDRIFT: return "energy drift above the set limit";
     default: return "unknown error";
   }
 }
 
-const char* mmp_last_error(void) { return g_last_error.c_str(); }
+const char* mmp_last_error(void) { return g_last_error; }
 
 const char* mmp_version(void) { return "mmp_b200 0.1.0 (sm_100a)"; }
 
 uint64_t mmp_kernel_launch_count(void) { return g_launches.load(); }
+
+int mmp_debug_fail_alloc(int64_t after) {
+  g_fail_after.store(after < 0 ? -1 : after);
+  return MMP_OK;
+}
+
+int64_t mmp_debug_live_allocations(void) { return g_live.load(); }
 
 }  // extern "C"
 

@@ -795,6 +795,12 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         *d.done_ctr = 0u;
         *d.step = n + 1;
         *d.total = total + 1;
+        if (d.drift_tol > 0.0 && d.monitors && total < d.mon_cap) {
+          // every CTA's energy sum is in (their adds precede their counter increments)
+          const double en = __ldcg(&d.energy[total]), e0 = *d.drift_ref;
+          if (e0 == 0.0) *d.drift_ref = en;
+          else if (!(fabs(en - e0) <= d.drift_tol * e0)) atomicOr(d.status, kStatusDrift);
+        }
         __threadfence();
       }
     }
@@ -1291,7 +1297,7 @@ __global__ void __launch_bounds__(256, (contract_min_blocks<T, DENSE>())) k_cont
   }
   // every thread polls with a bound; the barrier makes the outcome CTA-uniform and
   // also publishes the staged terms
-  const bool landed = mbar_wait(&bar, 0, kMaxWaitPolls);
+  const bool landed = mbar_wait(&bar, 0, d.tile_wait_polls);
   if (!__syncthreads_and(landed ? 1 : 0)) {
     if (threadIdx.x == 0) atomicOr(d.status, kStatusTimeout);
     // give the copies a second bounded chance to land before the CTA leaves
@@ -1474,7 +1480,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
     x.q = (T)tm.q;
     st[j] = x;
   }
-  const bool landed = mbar_wait(&bar, 0, kMaxWaitPolls);
+  const bool landed = mbar_wait(&bar, 0, d.tile_wait_polls);
   if (!__syncthreads_and(landed ? 1 : 0)) {
     if (threadIdx.x == 0) atomicOr(d.status, kStatusTimeout);
     mbar_wait(&bar, 0, kMaxWaitPolls);
@@ -1536,6 +1542,235 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
     if (idx >= nitems) continue;
     const int p = idx / H, tt = 2 * (idx - p * H);
     st2<T>(sigma + (size_t)p * nt + t0 + tt, mk<T>(acc[i][0], acc[i][1]), mk<T>(acc[i][2], acc[i][3]));
+  }
+}
+
+// ---- k_contract_sr: the term loop with the Raman recurrence run serially per pair field --
+// For tall tiles (more pair fields than k_contract holds in a tile). A CTA owns TB
+// consecutive samples of one solve and walks them in sub-blocks of kSrSub = 16 samples:
+//   staging  U of the next sub-block is loaded from global memory while this one is
+//            worked on, into a double buffer in which each sample pair (t, t + 1) of a
+//            row is stored as (Re t, Re t+1, Im t, Im t+1);
+//   phase A  each thread owns one or two pair fields q = (l, m) for the whole tile and runs
+//            the Raman recurrence S = lambda S + x (x = Re V and Im V, V = U_l conj(U_m))
+//            sample after sample from the state entering the tile (k_raman_carry); the
+//            state stays in registers from one sub-block to the next, and
+//            W_q = (1 - f_R) V + Im(kappa S) for the sub-block goes to shared memory
+//            (Raman off: W_q = V);
+//   phase B  sigma_p(t) = sum over p's merged terms of U_k (a Re W_q + i b Im W_q)
+//            (SolveDesc::sr_coef), one thread per (p, sample pair); the modes are laid out
+//            over the warps in descending term count, eight lanes per mode, so the lanes of
+//            a warp run loops of similar length.
+// Compared with the warp-per-field scan, a sample costs one step of each recurrence and no
+// scan levels. FP32 solves use the packed two-lane FMA (fma.rn.f32x2): phase A packs the
+// two recurrences (Re V and Im V share lambda), phase B the two samples of a pair; each
+// lane rounds exactly as the scalar FMA does. No asynchronous copies and no waits besides
+// __syncthreads.
+constexpr int kSrSub = 16;
+constexpr int kSrThreads = 256;
+constexpr int kSrPairsPerThread = 2;  // pair fields per thread: P <= 512
+constexpr int kSrMaxModes = 64;       // staging: M * kSrSub / 2 <= 2 kSrThreads
+
+__device__ __forceinline__ float2 pk_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pk_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ double2 pk_fma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 pk_mul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+
+// A sample pair (t, t + 1) of one row: re = (Re t, Re t+1), im = (Im t, Im t+1).
+template <typename T> struct SrPair {
+  c2<T> re, im;
+};
+template <typename T> __device__ __forceinline__ SrPair<T> ld_pair(const SrPair<T>* p) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    SrPair<T> r;
+    r.re = make_float2(v.x, v.y);
+    r.im = make_float2(v.z, v.w);
+    return r;
+  } else {
+    return *p;
+  }
+}
+template <typename T> __device__ __forceinline__ void st_pair(SrPair<T>* p, c2<T> re, c2<T> im) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(re.x, re.y, im.x, im.y);
+  } else {
+    p->re = re;
+    p->im = im;
+  }
+}
+// merged coefficient record of one term: FP32 (a, a, b, b), FP64 (a, b)
+template <typename T> struct SrCoef;
+template <> struct SrCoef<float> { using type = float4; };
+template <> struct SrCoef<double> { using type = double2; };
+
+// raman_mode: 0 Raman off, 2 the recurrence from the tile carries of k_raman_carry (tiles of TB)
+template <typename T>
+__global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
+    k_contract_sr(const SolveDesc* __restrict__ descs, int nt, int TB, int raman_mode) {
+  using V = c2<T>;
+  using SP = SrPair<T>;
+  using CF = typename SrCoef<T>::type;
+  constexpr int J = kSrSub / 2;  // sample pairs per sub-block
+  constexpr int RS = J + 1;      // row stride in sample pairs: consecutive rows start 16 bytes apart
+                                 // mod 128, so a quarter warp's rows fall on different banks
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SolveDesc& d = descs[blockIdx.y];
+  const int t0 = blockIdx.x * TB;
+  if (t0 >= nt || d.M == 0) return;               // empty slot
+  if (__ldcg(d.step) >= d.step_limit) return;     // finished solve (nothing is in flight yet)
+  const int M = d.M, P = d.P, nterm = d.sr_terms;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // shared memory: U [2][M][RS], W [P][RS], coefficients [nterm], k | q << 16 [nterm],
+  // term offsets [M + 1], mode order [M]
+  SP* sU = reinterpret_cast<SP*>(smem_raw);
+  SP* sW = sU + 2 * (size_t)M * RS;
+  CF* sCf = reinterpret_cast<CF*>(sW + (size_t)P * RS);
+  unsigned* sKq = reinterpret_cast<unsigned*>(sCf + nterm);
+  int* sOff = reinterpret_cast<int*>(sKq + nterm);
+  int* sPerm = sOff + (M + 1);
+  {
+    const CF* gCf = static_cast<const CF*>(d.sr_coef);
+    for (int i = tid; i < nterm; i += kSrThreads) {
+      sCf[i] = gCf[i];
+      sKq[i] = d.sr_kq[i];
+    }
+    for (int i = tid; i <= M; i += kSrThreads) sOff[i] = d.sr_off[i];
+    for (int i = tid; i < M; i += kSrThreads) sPerm[i] = d.sr_perm[i];
+  }
+  // U staging: sample pair j of row r is item r J + j; a thread carries at most two
+  const V* U = as_t2<T>(d.U);
+  const int nu = M * J;
+  V pre[2][2];
+  auto fetch = [&](int sub) {
+    const int ts = t0 + sub * kSrSub;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int idx = tid + r * kSrThreads;
+      if (idx < nu) {
+        const int row = idx / J, j = idx - row * J;
+        ld2<T>(U + (size_t)row * nt + ts + 2 * j, pre[r][0], pre[r][1]);
+      }
+    }
+  };
+  auto park = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int idx = tid + r * kSrThreads;
+      if (idx < nu) {
+        const int row = idx / J, j = idx - row * J;
+        st_pair<T>(sU + ((size_t)buf * M + row) * RS + j, mk<T>(pre[r][0].x, pre[r][1].x),
+                   mk<T>(pre[r][0].y, pre[r][1].y));
+      }
+    }
+  };
+  // phase A: this thread's pair fields and their recurrence states, packed as
+  // sr = (Re S_a, Re S_b), si = (Im S_a, Im S_b) (S_a for Re V, S_b for Im V)
+  int pl[kSrPairsPerThread], pm[kSrPairsPerThread];
+  V sr[kSrPairsPerThread], si[kSrPairsPerThread];
+  const int ntiles = nt / TB;
+#pragma unroll
+  for (int i = 0; i < kSrPairsPerThread; ++i) {
+    const int q = tid + i * kSrThreads;
+    pl[i] = pm[i] = 0;
+    sr[i] = si[i] = mk<T>(0, 0);
+    if (q < P) {
+      const int2 lm = d.pairs[q];
+      pl[i] = lm.x;
+      pm[i] = lm.y;
+      if (raman_mode == 2) {
+        const V* tiles = as_t2<T>(d.raman_tiles) + ((size_t)q * ntiles + blockIdx.x) * 2;
+        const V ca = tiles[0], cb = tiles[1];
+        sr[i] = mk<T>(ca.x, cb.x);
+        si[i] = mk<T>(ca.y, cb.y);
+      }
+    }
+  }
+  const T lr = (T)d.iir_lambda.x, li = (T)d.iir_lambda.y;
+  const V lr2 = mk<T>(lr, lr), li2 = mk<T>(li, li), nli2 = mk<T>(-li, -li);
+  const V kr2 = mk<T>((T)d.iir_kappa.x, (T)d.iir_kappa.x), ki2 = mk<T>((T)d.iir_kappa.y, (T)d.iir_kappa.y);
+  const T kerr = (T)d.one_minus_fR;
+  const V kerr2 = mk<T>(kerr, kerr);
+  V* sigma = as_t2<T>(d.sigma);
+  const int nsub = TB / kSrSub;
+  fetch(0);
+  park(0);
+  __syncthreads();  // U of sub-block 0, the terms
+  for (int sub = 0; sub < nsub; ++sub) {
+    const int buf = sub & 1;
+    if (sub + 1 < nsub) fetch(sub + 1);  // lands while this sub-block is worked on
+    const SP* uc = sU + (size_t)buf * M * RS;
+    // phase A
+#pragma unroll
+    for (int i = 0; i < kSrPairsPerThread; ++i) {
+      const int q = tid + i * kSrThreads;
+      if (q < P) {
+        const SP* ul = uc + pl[i] * RS;
+        const SP* um = uc + pm[i] * RS;
+        SP* wq = sW + (size_t)q * RS;
+        V Sr = sr[i], Si = si[i];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const SP a = ld_pair<T>(ul + j), b = ld_pair<T>(um + j);
+          V w[2];
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const V ue = e ? mk<T>(a.re.y, a.im.y) : mk<T>(a.re.x, a.im.x);
+            const V me = e ? mk<T>(b.re.y, b.im.y) : mk<T>(b.re.x, b.im.x);
+            const V x = cmulc(ue, me);  // V = U_l conj(U_m): (Re V, Im V)
+            if (raman_mode == 2) {
+              // S <- lambda S + x for both recurrences, then W = (1 - f_R) V + Im(kappa S)
+              const V t = pk_mul(li2, Sr);
+              Sr = pk_fma(lr2, Sr, pk_fma(nli2, Si, x));
+              Si = pk_fma(lr2, Si, t);
+              w[e] = pk_fma(kerr2, x, pk_fma(kr2, Si, pk_mul(ki2, Sr)));
+            } else {
+              w[e] = x;
+            }
+          }
+          st_pair<T>(wq + j, mk<T>(w[0].x, w[1].x), mk<T>(w[0].y, w[1].y));
+        }
+        sr[i] = Sr;
+        si[i] = Si;
+      }
+    }
+    __syncthreads();  // W of this sub-block is complete
+    // phase B
+    {
+      const int j = lane & 7;
+      const int ts = t0 + sub * kSrSub;
+      for (int gi = warp * 4 + (lane >> 3); gi < M; gi += (kSrThreads / 32) * 4) {
+        const int p = sPerm[gi];
+        V a1 = mk<T>(0, 0), a2 = a1, a3 = a1, a4 = a1;  // Re U Re X, Im U Im X, Re U Im X, Im U Re X
+        const int n1 = sOff[p + 1];
+#pragma unroll 2
+        for (int n = sOff[p]; n < n1; ++n) {
+          const CF c = sCf[n];
+          const unsigned kq = sKq[n];
+          const SP u = ld_pair<T>(uc + (kq & 0xffffu) * RS + j);
+          const SP w = ld_pair<T>(sW + (kq >> 16) * RS + j);
+          V aa, bb;
+          if constexpr (sizeof(T) == 4) {
+            aa = make_float2(c.x, c.y);
+            bb = make_float2(c.z, c.w);
+          } else {
+            aa = make_double2(c.x, c.x);
+            bb = make_double2(c.y, c.y);
+          }
+          const V xr = pk_mul(aa, w.re), xi = pk_mul(bb, w.im);  // X = a Re W + i b Im W
+          a1 = pk_fma(u.re, xr, a1);
+          a2 = pk_fma(u.im, xi, a2);
+          a3 = pk_fma(u.re, xi, a3);
+          a4 = pk_fma(u.im, xr, a4);
+        }
+        st2<T>(sigma + (size_t)p * nt + ts + 2 * j, mk<T>(a1.x - a2.x, a3.x + a4.x), mk<T>(a1.y - a2.y, a3.y + a4.y));
+      }
+    }
+    // buffer buf ^ 1 was last read in the previous sub-block, which ended at a barrier
+    if (sub + 1 < nsub) park(buf ^ 1);
+    __syncthreads();  // W is free again; the next U is in place
   }
 }
 
@@ -1601,7 +1836,9 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
     tc::relinquish();
   }
   tc::fence_before_sync();
-  bool ok = __syncthreads_and(mbar_wait(&bar_u, 0, kMaxWaitPolls) ? 1 : 0);
+  bool ok = __syncthreads_and(mbar_wait(&bar_u, 0, d.tile_wait_polls) ? 1 : 0);
+  const bool u_landed = ok;
+  int b_issued = -1;  // last chunk whose coefficient copy was issued
   tc::fence_after_sync();
   const uint32_t tmem = s_tmem;
   TileScan<float> ts;
@@ -1624,6 +1861,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
       mbar_arrive_expect_tx(&bar_b[buf], bbytes);
       bulk_g2s(B, d.dense_tc + (size_t)c * 4 * KC * N, bbytes, &bar_b[buf]);
     }
+    b_issued = c;
     for (int j = warp; j < KC; j += nwarps) {  // pair field q = c KC + j, one warp each
       const int q = c * KC + j;
       // lane L's samples 4L .. 4L + 3 of field j: one 16-byte chunk of each operand matrix
@@ -1659,6 +1897,7 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
     // the chunk's coefficients have landed and every thread's operand writes are done
     ok = __syncthreads_and(mbar_wait(&bar_b[buf], (c >> 1) & 1, kMaxWaitPolls) ? 1 : 0);
     if (!ok) break;
+    b_issued = -1;  // landed
     tc::fence_after_sync();
     if (tid == 0) {
       // Re: (A Re hi, B Re hi), (Re hi, Re lo), (Re lo, Re hi); Im likewise
@@ -1704,7 +1943,11 @@ __global__ void __launch_bounds__(512, 1) k_contract_tc(const SolveDesc* __restr
     }
   } else {
     if (tid == 0) atomicOr(d.status, kStatusTimeout);
-    if (committed >= 0) mbar_wait(&bar_m[committed & 1], (committed >> 1) & 1, kMaxWaitPolls);  // MMAs in flight
+    // nothing may still be writing this CTA's shared memory or TMEM when it leaves: the
+    // tile and coefficient copies in flight, the MMAs in flight (each waited for once more)
+    if (!u_landed) mbar_wait(&bar_u, 0, kMaxWaitPolls);
+    if (b_issued >= 0) mbar_wait(&bar_b[b_issued & 1], (b_issued >> 1) & 1, kMaxWaitPolls);
+    if (committed >= 0) mbar_wait(&bar_m[committed & 1], (committed >> 1) & 1, kMaxWaitPolls);
   }
   tc::fence_before_sync();
   __syncthreads();

@@ -71,7 +71,7 @@ def dropin_golden():
     CPU objects (oracle/_ref, from `make -C oracle`), run it, store its output."""
     import subprocess
     import tempfile
-    ref_dir = os.environ.get("REF_DIR", "/root/reference")
+    ref_dir = os.environ.get("REF_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
     objs = sorted(os.path.join(ROOT, "oracle", "_ref", f) for f in os.listdir(os.path.join(ROOT, "oracle", "_ref"))
                   if f.startswith("ref_") and f.endswith(".o") and f != "ref_driver.o")
     objs.append(os.path.join(ROOT, "oracle", "_ref", "fftw3_shim.o"))

@@ -283,20 +283,67 @@ def test_tensor_core_batch_members_match_single_solves(mmp):
 
 def test_raman_recurrence_in_tall_tiles(mmp, monkeypatch):
     # over 200 pair fields (328 with the reference's pair-slot mapping): U and all pair
-    # fields do not fit in a 64-sample tile, so the contraction holds the pair fields in
-    # chunks (k_contract_pc) with the recurrence still in the tiles; against the row scan
-    # (Raman rows through HBM) and the oracle
+    # fields do not fit in a 64-sample tile. Three routes: the serial recurrence per pair
+    # field in 16-sample sub-blocks (k_contract_sr, the default), the pair fields held in
+    # chunks with the warp-scan recurrence (k_contract_pc) and the row scan (Raman rows
+    # through HBM); against each other and the oracle
     prob = W.small_case(seed=97, M=26, nt=512, n_steps=3, nnz_target=1800)
+    ref = mo.solve(prob)
     for fl, tol in ((0, 2e-6), (capi.MMP_F_FP64, 1e-12)):
+        out_r, info_r = run(mmp, prob, [3], fl)
+        monkeypatch.setenv("MMP_CONTRACT_SR", "0")
         out_t, info_t = run(mmp, prob, [3], fl)
         monkeypatch.setenv("MMP_PAIR_CHUNK", "0")
         out_s, info_s = run(mmp, prob, [3], fl)
         monkeypatch.delenv("MMP_PAIR_CHUNK")
-        assert (info_t["raman_recurrence"], info_s["raman_recurrence"]) == (2, 1)
-        assert info_t["n_pair_fields"] > 200
-        assert 0 < info_t["contract_pair_chunk"] < info_t["n_pair_fields"] and info_s["contract_pair_chunk"] == 0
+        monkeypatch.delenv("MMP_CONTRACT_SR")
+        assert (info_r["raman_recurrence"], info_t["raman_recurrence"], info_s["raman_recurrence"]) == (2, 2, 1)
+        assert info_r["n_pair_fields"] > 200
+        assert info_r["contract_sub_block"] == 16 and info_r["contract_pair_chunk"] == 0
+        assert 0 < info_t["contract_pair_chunk"] < info_t["n_pair_fields"] and info_t["contract_sub_block"] == 0
+        assert info_s["contract_pair_chunk"] == 0 and info_s["contract_sub_block"] == 0
+        assert mo.rel_l2_per_mode(out_r, out_t).max() < tol
         assert mo.rel_l2_per_mode(out_t, out_s).max() < tol
-        assert mo.rel_l2_per_mode(out_t, mo.solve(prob)).max() < (TOL64 if fl else TOL32)
+        for out in (out_r, out_t):
+            assert mo.rel_l2_per_mode(out, ref).max() < (TOL64 if fl else TOL32)
+
+
+def _tall_case(seed, raman, M=22, nnz=1200, nt=256, n_steps=3):
+    # physical pair order (no pair-slot quirk), about 200 pair fields: a tall tile
+    return W.small_case(seed=seed, M=M, nt=nt, n_steps=n_steps, raman=raman, nnz_target=nnz,
+                        physical_order=True, peak_w=20.0)
+
+
+@pytest.mark.parametrize("raman", [True, False])
+@pytest.mark.parametrize("order", [4, 6])
+def test_serial_recurrence_contraction_against_oracle(mmp, monkeypatch, raman, order):
+    # k_contract_sr: Raman on (recurrence from the tile carries) and off (W = V), FP32 with
+    # the packed two-lane FMA and FP64; against the oracle and the term loop it replaces
+    prob = _tall_case(120 + order, raman).replace(method_order=order)
+    ref = mo.solve(prob)
+    for fl, tol in ((0, TOL32), (capi.MMP_F_FP64, TOL64)):
+        out, info = run(mmp, prob, [prob.n_steps], fl)
+        assert info["contract_sub_block"] == 16 and info["contract_tile"] == 256, info
+        assert info["n_pair_fields"] > 150
+        assert mo.rel_l2_per_mode(out, ref).max() < tol
+        monkeypatch.setenv("MMP_CONTRACT_SR", "0")
+        out_o, info_o = run(mmp, prob, [prob.n_steps], fl)
+        monkeypatch.delenv("MMP_CONTRACT_SR")
+        assert info_o["contract_sub_block"] == 0
+        assert mo.rel_l2_per_mode(out, out_o).max() < (2e-6 if fl == 0 else 1e-12)
+
+
+def test_serial_recurrence_batch_members_match_single_solves(mmp):
+    # members of different M and coupling in one batch, each a tall tile on its own too
+    # (so its single solve runs the same kernel): each CTA reads its own solve's merged
+    # terms, pairs and mode order
+    probs = [_tall_case(130, True), _tall_case(131, True, M=24, nnz=1500), _tall_case(134, True, M=23, nnz=1300)]
+    singles = [run(mmp, p, [3])[0] for p in probs]
+    with mmp.Batch(probs) as b:
+        b.propagate(3)
+        assert b.info(0)["contract_sub_block"] == 16
+        for i in range(len(probs)):
+            assert np.array_equal(b.result(i), singles[i]), i
 
 
 def test_dense_contraction_on_tensor_cores_16_modes(mmp, monkeypatch):
