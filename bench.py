@@ -448,7 +448,8 @@ def ours_arm(args, dist):
     chosen = {"row_ctas": info["cluster_ctas"], "raman_recurrence": info["raman_recurrence"],
               "dense_contraction": info["dense_contraction"], "graph_branches": info["graph_branches"],
               "tensor_core_contraction": info["tensor_core_contraction"],
-              "contract_pair_chunk": info["contract_pair_chunk"]}
+              "contract_pair_chunk": info["contract_pair_chunk"], "contract_sub_block": info["contract_sub_block"],
+              "contract_tile": info["contract_tile"], "autotuned": info["autotuned"]}
     if args.profile_only:
         print(json.dumps({"kernels_chosen": chosen}))
         batch.propagate(R)
@@ -526,8 +527,10 @@ def ours_arm(args, dist):
     flops = stage_flops(probe, n_pairs, n_terms, raman_path)
     tc = bool(info.get("tensor_core_contraction", 0))
     pc = bool(info.get("contract_pair_chunk", 0))
+    sr = bool(info.get("contract_sub_block", 0))
     names = {"pair": ("k_pair", "k_raman_scan", "k_raman_agg+k_raman_carry")[raman_path],
-             "contract": "k_contract_tc" if tc else ("k_contract_pc" if pc else "k_contract"), "nu": "k_nu"}
+             "contract": ("k_contract_tc" if tc else "k_contract_sr" if sr else "k_contract_pc" if pc
+                          else "k_contract"), "nu": "k_nu"}
     share = {k: prof[k]["ms_per_launch"] * prof[k]["launches"] for k in prof}
     tot = sum(share.values())
     dom = max(share, key=share.get)

@@ -123,7 +123,8 @@ typedef struct mmp_info {
   uint32_t autotuned;                       /* 1: cluster_ctas, contract_tile and graph_branches
                                                were chosen by timing steps of this batch on
                                                this device (or taken from that choice, cached
-                                               for the same shape) */
+                                               for the same shape); batches of one solve keep
+                                               the defaults the serving loop uses */
 } mmp_info;
 
 typedef struct mmp_solver mmp_solver;

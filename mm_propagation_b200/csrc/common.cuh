@@ -146,14 +146,15 @@ struct SolveDesc {
   // The contraction's terms merged per (p, k, pair field q) for k_contract_sr: a term
   // reading W_q and one reading conj(W_q) with the same k add up to
   //   U_k (a Re W_q + i b Im W_q),  a = Q1 + Q2, b = Q1 - Q2,
-  // sorted by p (sr_off[p] .. sr_off[p + 1]); sr_coef holds (a, a, b, b) in FP32 solves and
-  // (a, b) in FP64 ones, sr_kq = k | q << 16, sr_perm the modes by descending term count.
+  // sorted by p; sr_coef holds (a, b) in T, sr_kq = q | k << 16. sr_plan assigns the modes'
+  // term ranges to the kernel's groups of eight lanes, sr_rounds rounds of kSrGroups groups:
+  // (p, first term, end, role), role 0 a whole mode, 1 and 2 the lower and upper halves of a
+  // split one (the upper half hands its sums to the lower), 3 an empty group.
   const void* sr_coef;
   const unsigned* sr_kq;
-  const int* sr_off;   // [M + 1]
-  const int* sr_perm;  // [M]
+  const int4* sr_plan;
   int sr_terms;
-  int pad3_;
+  int sr_rounds;
 };
 
 // Largest mode count of the dense contraction form (its accumulators live in registers),

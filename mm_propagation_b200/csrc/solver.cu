@@ -347,7 +347,9 @@ struct Member {
   // offsets per p, modes by descending merged-term count
   std::vector<double> sr_ab;
   std::vector<unsigned> sr_kq;
-  std::vector<int> sr_off, sr_perm;
+  std::vector<int> sr_off;    // [M + 1]
+  std::vector<int4> sr_plan;  // k_contract_sr's group plan (SolveDesc::sr_plan)
+  int sr_rounds = 0;
   std::vector<double> poly;
   bool quirk = false;
   bool dense_ok = false;  // the dense contraction form is built for this solve
@@ -420,6 +422,50 @@ int validate(const mmp_params* p, std::string& why) {
   return MMP_OK;
 }
 
+// k_contract_sr's phase B plan: kSrGroups groups of eight lanes per round, as many rounds as
+// modes need. Groups left over after one per mode go to the modes with the most merged terms,
+// which are split in two halves in adjacent groups of one warp (pairs of groups 0-1 or 2-3);
+// the units are placed in descending term count so that groups of similar length share a
+// warp. Entry: (p, first term, end, role), role 0 whole, 1 lower half, 2 upper half, 3 empty.
+void sr_make_plan(Member& s) {
+  const int M = (int)s.M;
+  const int rounds = std::max(1, (M + kSrGroups - 1) / kSrGroups);
+  const int S = rounds * kSrGroups;
+  std::vector<int> order(M);
+  for (int q = 0; q < M; ++q) order[q] = q;
+  auto cnt = [&](int q) { return s.sr_off[q + 1] - s.sr_off[q]; };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cnt(x) > cnt(y); });
+  struct Unit { int p, n0, n1, halves, cost; };
+  std::vector<Unit> units;
+  int spare = S - M;
+  for (int q : order) {
+    const bool split = spare > 0 && cnt(q) >= 2;
+    if (split) --spare;
+    units.push_back({q, s.sr_off[q], s.sr_off[q + 1], split ? 2 : 1, split ? (cnt(q) + 1) / 2 : cnt(q)});
+  }
+  std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.cost > b.cost; });
+  s.sr_plan.assign(S, make_int4(0, 0, 0, 3));
+  std::vector<char> used(S, 0);
+  for (const Unit& u : units) {
+    int slot = -1;
+    if (u.halves == 2)
+      for (int g = 0; g + 1 < S && slot < 0; g += 2)
+        if (!used[g] && !used[g + 1]) slot = g;
+    if (slot >= 0) {
+      const int mid = u.n0 + (u.n1 - u.n0 + 1) / 2;
+      s.sr_plan[slot] = make_int4(u.p, u.n0, mid, 1);
+      s.sr_plan[slot + 1] = make_int4(u.p, mid, u.n1, 2);
+      used[slot] = used[slot + 1] = 1;
+      continue;
+    }
+    for (int g = 0; g < S && slot < 0; ++g)  // whole (also a split that found no aligned pair)
+      if (!used[g]) slot = g;
+    s.sr_plan[slot] = make_int4(u.p, u.n0, u.n1, 0);
+    used[slot] = 1;
+  }
+  s.sr_rounds = rounds;
+}
+
 // The reference's setup, in FP64 with the same expressions.
 void host_setup(const mmp_params* p, Member& s) {
   const uint32_t M = p->n_modes, L = p->n_beta;
@@ -479,27 +525,39 @@ void host_setup(const mmp_params* p, Member& s) {
     if (s.unique_pairs[i] != i) s.quirk = !physical;
   // contraction terms with the pair each one actually reads
   // (reference CPU: V[slot] = U[slot % M] conj(U[slot / M]), :126-133, :195-205)
+  auto pair_of = [&](const mmp_nz* e, int& le, int& me) {
+    const uint32_t code = e->l + e->m * M;
+    const uint32_t src = physical ? code : slot_of[code];
+    le = (int)(src % M);
+    me = (int)(src / M);
+    return std::make_pair(std::min(le, me), std::max(le, me));
+  };
+  // the pair fields the non-zero terms read, numbered in (l, m) order: neighbouring pair
+  // fields then mostly share l and have distinct m, which keeps the one-pair-field-per-lane
+  // loads of k_contract_sr and k_raman_agg_sr free of shared-memory bank conflicts
   std::map<std::pair<int, int>, int> pair_idx;
+  for (uint32_t q = 0; q < M; ++q)
+    for (const mmp_nz* e : byp[q]) {
+      int le, me;
+      if (e->value != 0.0) pair_idx[pair_of(e, le, me)] = 0;
+    }
+  for (auto& kv : pair_idx) {
+    kv.second = (int)s.pairs.size();
+    s.pairs.push_back(make_int2(kv.first.first, kv.first.second));
+  }
   s.term_off.assign(M + 1, 0);
   for (uint32_t q = 0; q < M; ++q) {
     s.term_off[q] = (int)s.terms.size();
     for (const mmp_nz* e : byp[q]) {
       if (e->value == 0.0) continue;  // contributes exactly 0
-      const uint32_t code = e->l + e->m * M;
-      const uint32_t src = physical ? code : slot_of[code];
-      const int le = (int)(src % M), me = (int)(src / M);
-      const int lo = std::min(le, me), hi = std::max(le, me);
-      auto key = std::make_pair(lo, hi);
-      if (!pair_idx.count(key)) {
-        pair_idx[key] = (int)s.pairs.size();
-        s.pairs.push_back(make_int2(lo, hi));
-      }
+      int le, me;
+      const int idx = pair_idx[pair_of(e, le, me)];
       Term t;
       t.k = (unsigned short)e->k;
       t.l = (unsigned short)le;
       t.m = (unsigned short)me;
-      t.pc = (unsigned short)(pair_idx[key] | (le > me ? 0x8000 : 0));  // R_ml = conj(R_lm): h_R is real
-      t.q = e->value / max_Q;                                           // Q_tilde (:117-136)
+      t.pc = (unsigned short)(idx | (le > me ? 0x8000 : 0));  // R_ml = conj(R_lm): h_R is real
+      t.q = e->value / max_Q;                                  // Q_tilde (:117-136)
       s.terms.push_back(t);
     }
     // each p's terms in pair-field order (stable): the pair-chunked contraction walks
@@ -515,10 +573,10 @@ void host_setup(const mmp_params* p, Member& s) {
   s.sr_off.assign(M + 1, 0);
   for (uint32_t q = 0; q < M; ++q) {
     s.sr_off[q] = (int)s.sr_kq.size();
-    std::map<std::pair<int, int>, std::pair<double, double>> merged;  // (pair, k) -> (a, b)
+    std::map<std::pair<int, int>, std::pair<double, double>> merged;  // (k, pair) -> (a, b)
     for (int j = s.term_off[q]; j < s.term_off[q + 1]; ++j) {
       const Term& t = s.terms[j];
-      auto& ab = merged[std::make_pair((int)(t.pc & 0x7fff), (int)t.k)];
+      auto& ab = merged[std::make_pair((int)t.k, (int)(t.pc & 0x7fff))];
       ab.first += t.q;
       ab.second += (t.pc & 0x8000) ? -t.q : t.q;
     }
@@ -529,11 +587,7 @@ void host_setup(const mmp_params* p, Member& s) {
     }
   }
   s.sr_off[M] = (int)s.sr_kq.size();
-  s.sr_perm.resize(M);
-  for (uint32_t q = 0; q < M; ++q) s.sr_perm[q] = (int)q;
-  std::stable_sort(s.sr_perm.begin(), s.sr_perm.end(), [&](int x, int y) {
-    return s.sr_off[x + 1] - s.sr_off[x] > s.sr_off[y + 1] - s.sr_off[y];
-  });
+  sr_make_plan(s);
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -721,9 +775,16 @@ int launch_pairs(mmp_batch* b, const KernelSet& ks, int nsolves, int stage, cons
     int TT = b->TT;
     const SolveDesc* dd = descs;
     void* args[] = {(void*)&dd, &nt, &TT};
-    const int smem = (int)(((size_t)b->Mmax * TT + TT) * t2);  // U tile and the weight table
-    const void* fa = b->fp64 ? (const void*)&k_raman_agg<double> : (const void*)&k_raman_agg<float>;
-    CUDA_TRY(launch(fa, dim3((unsigned)(nt / TT), (unsigned)nsolves, 1), 256, smem, 1, st ? st : b->stream, args));
+    if (b->sr) {  // one thread per pair field through the tile (k_contract_sr's tiles)
+      const int smem = (int)(2 * (size_t)b->Mmax * (kSrSub / 2 + 1) * 2 * t2);
+      const void* fa = b->fp64 ? (const void*)&k_raman_agg_sr<double> : (const void*)&k_raman_agg_sr<float>;
+      CUDA_TRY(launch(fa, dim3((unsigned)(nt / TT), (unsigned)nsolves, 1), kSrThreads, smem, 1,
+                      st ? st : b->stream, args));
+    } else {
+      const int smem = (int)(((size_t)b->Mmax * TT + TT) * t2);  // U tile and the weight table
+      const void* fa = b->fp64 ? (const void*)&k_raman_agg<double> : (const void*)&k_raman_agg<float>;
+      CUDA_TRY(launch(fa, dim3((unsigned)(nt / TT), (unsigned)nsolves, 1), 256, smem, 1, st ? st : b->stream, args));
+    }
     const void* fc = b->fp64 ? (const void*)&k_raman_carry<double> : (const void*)&k_raman_carry<float>;
     CUDA_TRY(launch(fc, dim3((unsigned)b->Pmax, (unsigned)nsolves, 1), 32, 0, 1, st ? st : b->stream, args));
     return MMP_OK;
@@ -932,6 +993,9 @@ int batch_open(mmp_batch* b, const mmp_params* p0, const Tableau& tab0) {
   b->logn = ilog2_exact(p0->nt);
   b->tab = tab0;
   b->ks = kernels_for(b->fp64 ? 1 : 0, b->logn);
+  if (const char* env = std::getenv("MMP_ROW_SPLIT"))  // 1: rows split over twice the CTAs, where built
+    if (std::atoi(env) == 1 && kernels_for(b->fp64 ? 1 : 0, b->logn, 1).prime)
+      b->ks = kernels_for(b->fp64 ? 1 : 0, b->logn, 1);
   b->ks64 = kernels_for(1, b->logn);
   if (!b->ks.prime || !b->ks64.prime) return fail(MMP_ENOTSUP, "no kernels built for this nt");
   b->kernels_per_step = b->tab.s * ((b->raman ? 1 : 0) + 2);
@@ -1026,7 +1090,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   off = align_up(off + (M + 1) * sizeof(int));
   off = align_up(off + std::max<size_t>(s.sr_kq.size(), 1) * 16);                // merged coefficients
   off = align_up(off + std::max<size_t>(s.sr_kq.size(), 1) * sizeof(unsigned));  // their k | q << 16
-  off = align_up(off + (2 * M + 1) * sizeof(int));                               // offsets, mode order
+  off = align_up(off + s.sr_plan.size() * sizeof(int4));                         // group plan
   off = align_up(off + kCounterWords * sizeof(unsigned long long));
   return off;
 }
@@ -1094,7 +1158,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   const size_t nsr = s.sr_kq.size();
   const size_t o_src = off; off = align_up(off + std::max<size_t>(nsr, 1) * 16);
   const size_t o_skq = off; off = align_up(off + std::max<size_t>(nsr, 1) * sizeof(unsigned));
-  const size_t o_soff = off; off = align_up(off + (2 * M + 1) * sizeof(int));
+  const size_t o_splan = off; off = align_up(off + s.sr_plan.size() * sizeof(int4));
   const size_t o_cnt = off; off = align_up(off + kCounterWords * sizeof(unsigned long long));
   cudaError_t e = dev_malloc(&s.block, off, b->mempool, b->stream);
   if (e != cudaSuccess) {
@@ -1135,9 +1199,9 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.term_off = (const int*)T2ptr(s.block, o_toff);
   d.sr_coef = T2ptr(s.block, o_src);
   d.sr_kq = (const unsigned*)T2ptr(s.block, o_skq);
-  d.sr_off = (const int*)T2ptr(s.block, o_soff);
-  d.sr_perm = d.sr_off + (M + 1);
+  d.sr_plan = (const int4*)T2ptr(s.block, o_splan);
   d.sr_terms = (int)nsr;
+  d.sr_rounds = s.sr_rounds;
   s.counters = (unsigned long long*)T2ptr(s.block, o_cnt);
   d.step = s.counters;
   d.total = s.counters + 1;
@@ -1186,25 +1250,17 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
     CUDA_TRY(cudaMemcpyAsync((void*)d.terms, s.terms.data(), s.terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync((void*)d.term_off, s.term_off.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   {
-    // merged terms (k_contract_sr): FP32 records (a, a, b, b), FP64 records (a, b)
+    // merged terms (k_contract_sr): records (a, b) in T
     std::vector<float> cf32;
-    if (!b->fp64) {
-      cf32.resize(4 * nsr);
-      for (size_t i = 0; i < nsr; ++i) {
-        cf32[4 * i] = cf32[4 * i + 1] = (float)s.sr_ab[2 * i];
-        cf32[4 * i + 2] = cf32[4 * i + 3] = (float)s.sr_ab[2 * i + 1];
-      }
-    }
-    std::vector<int> offs(s.sr_off);
-    offs.insert(offs.end(), s.sr_perm.begin(), s.sr_perm.end());
+    if (!b->fp64) cf32.assign(s.sr_ab.begin(), s.sr_ab.end());
     if (nsr) {
       CUDA_TRY(cudaMemcpyAsync((void*)d.sr_coef, b->fp64 ? (const void*)s.sr_ab.data() : (const void*)cf32.data(),
-                               nsr * 16, cudaMemcpyHostToDevice, b->stream));
+                               nsr * t2, cudaMemcpyHostToDevice, b->stream));
       CUDA_TRY(cudaMemcpyAsync((void*)d.sr_kq, s.sr_kq.data(), nsr * sizeof(unsigned), cudaMemcpyHostToDevice,
                                b->stream));
     }
-    CUDA_TRY(cudaMemcpyAsync((void*)d.sr_off, offs.data(), offs.size() * sizeof(int), cudaMemcpyHostToDevice,
-                             b->stream));
+    CUDA_TRY(cudaMemcpyAsync((void*)d.sr_plan, s.sr_plan.data(), s.sr_plan.size() * sizeof(int4),
+                             cudaMemcpyHostToDevice, b->stream));
     CUDA_TRY(cudaStreamSynchronize(b->stream));  // the staging vectors are host temporaries
   }
   if (s.dense_ok) {
@@ -1294,7 +1350,10 @@ bool batch_shape(mmp_batch* b) {
   while (TT > 32 && (size_t)rows * TT * t2 > 100 * 1024) TT >>= 1;
   while (TT > 2 && (size_t)rows * TT * t2 > 200 * 1024) TT >>= 1;  // >= 2: 16-byte bulk copies
   while (TT > (int)b->nt) TT >>= 1;
-  if (b->tile_req >= 64 && b->tile_req < TT) TT = b->tile_req;  // a smaller tile the autotuner times
+  int tile_req = b->tile_req;  // the autotuner's tile, else MMP_CONTRACT_TILE
+  if (!tile_req)
+    if (const char* env = std::getenv("MMP_CONTRACT_TILE")) tile_req = std::atoi(env);
+  if (tile_req >= 64 && tile_req < TT) TT = tile_req;
   size_t smem = (size_t)rows * TT * t2;
   if (const char* env = std::getenv("MMP_RAMAN_FFT"))  // 1 forces the FFT convolution
     if (std::atoi(env) == 1) iir = false;
@@ -1367,12 +1426,12 @@ bool batch_shape(mmp_batch* b) {
       if (std::atoi(env) == 0 && b->raman) ok = false;
     const size_t sp = 2 * t2;  // one sample pair of one row
     const size_t rs = kSrSub / 2 + 1;
-    const size_t need = (2 * (size_t)Mmax + (size_t)Pall) * rs * sp + max_sr_terms * (16 + sizeof(unsigned)) +
-                        (2 * (size_t)Mmax + 1) * sizeof(int);
+    const size_t plan = (size_t)((Mmax + kSrGroups - 1) / kSrGroups) * kSrGroups * sizeof(int4);
+    const size_t need = (2 * (size_t)Mmax + (size_t)Pall) * rs * sp + plan + max_sr_terms * (t2 + sizeof(unsigned));
     if (ok && need <= 227 * 1024) {
       sr = true;
       pchunk = 0;
-      TT = std::min(b->tile_req >= 64 ? std::min(b->tile_req, 256) : 256, (int)b->nt);
+      TT = std::min(tile_req >= 64 ? std::min(tile_req, 256) : 256, (int)b->nt);
       fused = b->raman;
       smem = (need + 15) & ~(size_t)15;
     }
@@ -1418,8 +1477,10 @@ bool batch_shape(mmp_batch* b) {
 // The timed steps advance the solves; afterwards every member gets its initial fields
 // back at z = 0 with its counters cleared, as if nothing had run. The choice is cached
 // per shape (device, precision, NT, tableau size, largest M and P, batch size, Raman,
-// contraction form). MMP_ROW_SPLIT, MMP_CONTRACT_TILE and MMP_GROUPS each fix one
-// parameter instead.
+// contraction form, candidate lists). Batches of one solve are not tuned: they keep the
+// default parameters, the ones the serving loop's pools use, so that a served solve and
+// the same solve run alone give the same bits. MMP_ROW_SPLIT, MMP_CONTRACT_TILE and
+// MMP_GROUPS each fix one parameter instead.
 struct TuneChoice {
   int xc = 0, tile = 0, groups = 1;
 };
@@ -1498,13 +1559,17 @@ int autotune(mmp_batch* b, const mmp_params* const* params) {
   c.tile = tiles[0];
   c.groups = gs[0];
   b->tuned = 0;
-  if (xcs.size() == 1 && tiles.size() == 1 && gs.size() == 1) {
+  if (b->span < 2 || (xcs.size() == 1 && tiles.size() == 1 && gs.size() == 1)) {
     apply(c);
     return MMP_OK;
   }
-  const std::vector<int> key = {b->device, b->fp64 ? 1 : 0, b->logn, b->tab.s, b->Mmax, b->Pmax,
-                                (int)b->span, b->raman ? 1 : 0, b->tc ? 1 : 0, b->sr ? 1 : 0,
-                                b->pchunk ? 1 : 0, b->dense, (int)xcs.size(), (int)tiles.size(), (int)gs.size()};
+  std::vector<int> key = {b->device, b->fp64 ? 1 : 0, b->logn, b->tab.s, b->Mmax, b->Pmax,
+                          (int)b->span, b->raman ? 1 : 0, b->tc ? 1 : 0, b->sr ? 1 : 0,
+                          b->pchunk ? 1 : 0, b->dense, -1};
+  for (const std::vector<int>* v : {&xcs, &tiles, &gs}) {
+    key.insert(key.end(), v->begin(), v->end());
+    key.push_back(-1);
+  }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);

@@ -1558,9 +1558,13 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2)) k_contract_pc(c
 //            W_q = (1 - f_R) V + Im(kappa S) for the sub-block goes to shared memory
 //            (Raman off: W_q = V);
 //   phase B  sigma_p(t) = sum over p's merged terms of U_k (a Re W_q + i b Im W_q)
-//            (SolveDesc::sr_coef), one thread per (p, sample pair); the modes are laid out
-//            over the warps in descending term count, eight lanes per mode, so the lanes of
-//            a warp run loops of similar length.
+//            (SolveDesc::sr_coef), eight lanes (one per sample pair) per group; a plan
+//            made on the host (SolveDesc::sr_plan) gives each group a mode, or half of a
+//            mode with many terms (the two halves sit in one warp and are added by a
+//            shuffle), so the longest group's term loop is about half as long as the
+//            heaviest mode's; groups of similar length share a warp.
+// Per term a lane reads U_k and W_q (16 bytes each for its two samples) and the 8-byte
+// coefficient from shared memory, whose bandwidth bounds the kernel.
 // Compared with the warp-per-field scan, a sample costs one step of each recurrence and no
 // scan levels. FP32 solves use the packed two-lane FMA (fma.rn.f32x2): phase A packs the
 // two recurrences (Re V and Im V share lambda), phase B the two samples of a pair; each
@@ -1601,10 +1605,13 @@ template <typename T> __device__ __forceinline__ void st_pair(SrPair<T>* p, c2<T
     p->im = im;
   }
 }
-// merged coefficient record of one term: FP32 (a, a, b, b), FP64 (a, b)
-template <typename T> struct SrCoef;
-template <> struct SrCoef<float> { using type = float4; };
-template <> struct SrCoef<double> { using type = double2; };
+constexpr int kSrGroups = (kSrThreads / 32) * 4;  // groups of eight lanes in phase B
+
+template <typename V> __device__ __forceinline__ V shfl_down_c(V v, int d) {
+  v.x = __shfl_down_sync(0xffffffffu, v.x, d);
+  v.y = __shfl_down_sync(0xffffffffu, v.y, d);
+  return v;
+}
 
 // raman_mode: 0 Raman off, 2 the recurrence from the tile carries of k_raman_carry (tiles of TB)
 template <typename T>
@@ -1612,7 +1619,7 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
     k_contract_sr(const SolveDesc* __restrict__ descs, int nt, int TB, int raman_mode) {
   using V = c2<T>;
   using SP = SrPair<T>;
-  using CF = typename SrCoef<T>::type;
+  using CF = c2<T>;              // merged coefficient (a, b)
   constexpr int J = kSrSub / 2;  // sample pairs per sub-block
   constexpr int RS = J + 1;      // row stride in sample pairs: consecutive rows start 16 bytes apart
                                  // mod 128, so a quarter warp's rows fall on different banks
@@ -1621,24 +1628,22 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
   const int t0 = blockIdx.x * TB;
   if (t0 >= nt || d.M == 0) return;               // empty slot
   if (__ldcg(d.step) >= d.step_limit) return;     // finished solve (nothing is in flight yet)
-  const int M = d.M, P = d.P, nterm = d.sr_terms;
+  const int M = d.M, P = d.P, nterm = d.sr_terms, rounds = d.sr_rounds;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // shared memory: U [2][M][RS], W [P][RS], coefficients [nterm], k | q << 16 [nterm],
-  // term offsets [M + 1], mode order [M]
+  // shared memory: U [2][M][RS], W [P][RS], group plan [rounds kSrGroups], coefficients
+  // [nterm], q | k << 16 [nterm]
   SP* sU = reinterpret_cast<SP*>(smem_raw);
   SP* sW = sU + 2 * (size_t)M * RS;
-  CF* sCf = reinterpret_cast<CF*>(sW + (size_t)P * RS);
+  int4* sPlan = reinterpret_cast<int4*>(sW + (size_t)P * RS);
+  CF* sCf = reinterpret_cast<CF*>(sPlan + rounds * kSrGroups);
   unsigned* sKq = reinterpret_cast<unsigned*>(sCf + nterm);
-  int* sOff = reinterpret_cast<int*>(sKq + nterm);
-  int* sPerm = sOff + (M + 1);
   {
     const CF* gCf = static_cast<const CF*>(d.sr_coef);
     for (int i = tid; i < nterm; i += kSrThreads) {
       sCf[i] = gCf[i];
       sKq[i] = d.sr_kq[i];
     }
-    for (int i = tid; i <= M; i += kSrThreads) sOff[i] = d.sr_off[i];
-    for (int i = tid; i < M; i += kSrThreads) sPerm[i] = d.sr_perm[i];
+    for (int i = tid; i < rounds * kSrGroups; i += kSrThreads) sPlan[i] = d.sr_plan[i];
   }
   // U staging: sample pair j of row r is item r J + j; a thread carries at most two
   const V* U = as_t2<T>(d.U);
@@ -1741,36 +1746,144 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
     {
       const int j = lane & 7;
       const int ts = t0 + sub * kSrSub;
-      for (int gi = warp * 4 + (lane >> 3); gi < M; gi += (kSrThreads / 32) * 4) {
-        const int p = sPerm[gi];
-        V a1 = mk<T>(0, 0), a2 = a1, a3 = a1, a4 = a1;  // Re U Re X, Im U Im X, Re U Im X, Im U Re X
-        const int n1 = sOff[p + 1];
+      for (int r = 0; r < rounds; ++r) {
+        const int4 pl = sPlan[r * kSrGroups + warp * 4 + (lane >> 3)];  // p, first term, end, role
+        // sigma = U X summed over the terms: Re = a1 - a2, Im = a3 + a4 with a1 = sum Re U Re X,
+        // a2 = sum Im U Im X, a3 = sum Re U Im X, a4 = sum Im U Re X (packed over the pair)
+        V a1 = mk<T>(0, 0), a2 = a1, a3 = a1, a4 = a1;
 #pragma unroll 2
-        for (int n = sOff[p]; n < n1; ++n) {
-          const CF c = sCf[n];
+        for (int n = pl.y; n < pl.z; ++n) {
           const unsigned kq = sKq[n];
-          const SP u = ld_pair<T>(uc + (kq & 0xffffu) * RS + j);
-          const SP w = ld_pair<T>(sW + (kq >> 16) * RS + j);
-          V aa, bb;
-          if constexpr (sizeof(T) == 4) {
-            aa = make_float2(c.x, c.y);
-            bb = make_float2(c.z, c.w);
-          } else {
-            aa = make_double2(c.x, c.x);
-            bb = make_double2(c.y, c.y);
-          }
-          const V xr = pk_mul(aa, w.re), xi = pk_mul(bb, w.im);  // X = a Re W + i b Im W
+          const CF c = sCf[n];
+          const SP u = ld_pair<T>(uc + (kq >> 16) * RS + j);
+          const SP w = ld_pair<T>(sW + (kq & 0xffffu) * RS + j);
+          const V xr = pk_mul(mk<T>(c.x, c.x), w.re), xi = pk_mul(mk<T>(c.y, c.y), w.im);  // X
           a1 = pk_fma(u.re, xr, a1);
           a2 = pk_fma(u.im, xi, a2);
           a3 = pk_fma(u.re, xi, a3);
           a4 = pk_fma(u.im, xr, a4);
         }
-        st2<T>(sigma + (size_t)p * nt + ts + 2 * j, mk<T>(a1.x - a2.x, a3.x + a4.x), mk<T>(a1.y - a2.y, a3.y + a4.y));
+        // the upper half of a split mode (the next group, 8 lanes up) adds into the lower half
+        const V b1 = shfl_down_c(a1, 8), b2 = shfl_down_c(a2, 8), b3 = shfl_down_c(a3, 8), b4 = shfl_down_c(a4, 8);
+        if (pl.w == 1) {
+          a1 = cadd(a1, b1);
+          a2 = cadd(a2, b2);
+          a3 = cadd(a3, b3);
+          a4 = cadd(a4, b4);
+        }
+        if (pl.w <= 1)
+          st2<T>(sigma + (size_t)pl.x * nt + ts + 2 * j, mk<T>(a1.x - a2.x, a3.x + a4.x), mk<T>(a1.y - a2.y, a3.y + a4.y));
       }
     }
     // buffer buf ^ 1 was last read in the previous sub-block, which ended at a barrier
     if (sub + 1 < nsub) park(buf ^ 1);
     __syncthreads();  // W is free again; the next U is in place
+  }
+}
+
+// ---- k_raman_agg_sr: the tile aggregates for k_contract_sr's tiles ------------------------
+// One thread per pair field: the aggregate of the recurrence over the tile from a zero
+// start, S_end = sum_t lambda^(TB-1-t) x_t (x = Re V, Im V, V = U_l conj(U_m)), run as
+// S <- lambda S + x sample after sample (the arithmetic of k_contract_sr's phase A without
+// the output), U arriving in sub-blocks of kSrSub samples through the same double buffer.
+// k_raman_carry turns the aggregates into the states entering the tiles.
+template <typename T>
+__global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 4 : 2))
+    k_raman_agg_sr(const SolveDesc* __restrict__ descs, int nt, int TB) {
+  using V = c2<T>;
+  using SP = SrPair<T>;
+  constexpr int J = kSrSub / 2;
+  constexpr int RS = J + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SolveDesc& d = descs[blockIdx.y];
+  const int t0 = blockIdx.x * TB;
+  if (t0 >= nt || d.M == 0) return;            // empty slot
+  if (__ldcg(d.step) >= d.step_limit) return;  // finished solve
+  const int M = d.M, P = d.P, tid = threadIdx.x;
+  SP* sU = reinterpret_cast<SP*>(smem_raw);  // [2][M][RS]
+  const V* U = as_t2<T>(d.U);
+  const int nu = M * J;
+  V pre[2][2];
+  auto fetch = [&](int sub) {
+    const int ts = t0 + sub * kSrSub;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int idx = tid + r * kSrThreads;
+      if (idx < nu) {
+        const int row = idx / J, j = idx - row * J;
+        ld2<T>(U + (size_t)row * nt + ts + 2 * j, pre[r][0], pre[r][1]);
+      }
+    }
+  };
+  auto park = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int idx = tid + r * kSrThreads;
+      if (idx < nu) {
+        const int row = idx / J, j = idx - row * J;
+        st_pair<T>(sU + ((size_t)buf * M + row) * RS + j, mk<T>(pre[r][0].x, pre[r][1].x),
+                   mk<T>(pre[r][0].y, pre[r][1].y));
+      }
+    }
+  };
+  int pl[kSrPairsPerThread], pm[kSrPairsPerThread];
+  V sr[kSrPairsPerThread], si[kSrPairsPerThread];
+#pragma unroll
+  for (int i = 0; i < kSrPairsPerThread; ++i) {
+    const int q = tid + i * kSrThreads;
+    pl[i] = pm[i] = 0;
+    sr[i] = si[i] = mk<T>(0, 0);
+    if (q < P) {
+      const int2 lm = d.pairs[q];
+      pl[i] = lm.x;
+      pm[i] = lm.y;
+    }
+  }
+  const T lr = (T)d.iir_lambda.x, li = (T)d.iir_lambda.y;
+  const V lr2 = mk<T>(lr, lr), li2 = mk<T>(li, li), nli2 = mk<T>(-li, -li);
+  const int nsub = TB / kSrSub;
+  fetch(0);
+  park(0);
+  __syncthreads();
+  for (int sub = 0; sub < nsub; ++sub) {
+    const int buf = sub & 1;
+    if (sub + 1 < nsub) fetch(sub + 1);
+    const SP* uc = sU + (size_t)buf * M * RS;
+#pragma unroll
+    for (int i = 0; i < kSrPairsPerThread; ++i) {
+      if (tid + i * kSrThreads < P) {
+        const SP* ul = uc + pl[i] * RS;
+        const SP* um = uc + pm[i] * RS;
+        V Sr = sr[i], Si = si[i];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const SP a = ld_pair<T>(ul + j), b = ld_pair<T>(um + j);
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const V x = cmulc(e ? mk<T>(a.re.y, a.im.y) : mk<T>(a.re.x, a.im.x),
+                              e ? mk<T>(b.re.y, b.im.y) : mk<T>(b.re.x, b.im.x));
+            const V t = pk_mul(li2, Sr);
+            Sr = pk_fma(lr2, Sr, pk_fma(nli2, Si, x));
+            Si = pk_fma(lr2, Si, t);
+          }
+        }
+        sr[i] = Sr;
+        si[i] = Si;
+      }
+    }
+    // buffer buf ^ 1 was last read in the previous sub-block, which ended at this barrier
+    if (sub + 1 < nsub) park(buf ^ 1);
+    __syncthreads();
+  }
+  const int ntiles = nt / TB;
+  V* out = as_t2<T>(d.raman_tiles);
+#pragma unroll
+  for (int i = 0; i < kSrPairsPerThread; ++i) {
+    const int q = tid + i * kSrThreads;
+    if (q < P) {
+      out[((size_t)q * ntiles + blockIdx.x) * 2] = mk<T>(sr[i].x, si[i].x);      // Re V recurrence
+      out[((size_t)q * ntiles + blockIdx.x) * 2 + 1] = mk<T>(sr[i].y, si[i].y);  // Im V recurrence
+    }
   }
 }
 

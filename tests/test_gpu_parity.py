@@ -20,6 +20,16 @@ TOL64 = 1e-11
 TOL32 = 1e-5
 
 
+@pytest.fixture
+def pinned(monkeypatch):
+    """The launch parameters the autotuner picks for batches (row split, contraction tile,
+    graph branches), fixed to the defaults single solves use: batch members and single
+    solves then run the same kernels and give the same bits."""
+    monkeypatch.setenv("MMP_ROW_SPLIT", "0")
+    monkeypatch.setenv("MMP_CONTRACT_TILE", "256")
+    monkeypatch.setenv("MMP_GROUPS", "1")
+
+
 def run(mmp, prob, chunks, flags=0):
     prob = prob.replace(flags=prob.flags | flags)
     with mmp.Solver(prob) as s:
@@ -88,7 +98,7 @@ def test_continuous_chunks_equal_one_call(mmp):
     assert mo.rel_l2_per_mode(reset, one).max() > 1e-8
 
 
-def test_batch_members_match_single_solves(mmp):
+def test_batch_members_match_single_solves(mmp, pinned):
     probs = [W.small_case(seed=60 + i, M=m, nt=512, n_steps=10, nnz_target=8 + 4 * i)
              for i, m in enumerate([2, 3, 1, 4])]
     probs = [p.replace(flags=capi.MMP_F_FP64) for p in probs]
@@ -270,7 +280,7 @@ def test_dense_contraction_on_tensor_cores_15_modes(mmp, monkeypatch):
     assert mo.rel_l2_per_mode(out_t, out_s).max() < 2e-6
 
 
-def test_tensor_core_batch_members_match_single_solves(mmp):
+def test_tensor_core_batch_members_match_single_solves(mmp, pinned):
     # solves of different M in one batch: each tile's MMA shape comes from its own solve
     probs = [_dense_case(96 + i, m, 512, 5, True) for i, m in enumerate([6, 8, 7])]
     singles = [run(mmp, p, [5])[0] for p in probs]
@@ -333,7 +343,7 @@ def test_serial_recurrence_contraction_against_oracle(mmp, monkeypatch, raman, o
         assert mo.rel_l2_per_mode(out, out_o).max() < (2e-6 if fl == 0 else 1e-12)
 
 
-def test_serial_recurrence_batch_members_match_single_solves(mmp):
+def test_serial_recurrence_batch_members_match_single_solves(mmp, pinned):
     # members of different M and coupling in one batch, each a tall tile on its own too
     # (so its single solve runs the same kernel): each CTA reads its own solve's merged
     # terms, pairs and mode order
