@@ -308,6 +308,23 @@ def tf32_peak_tflops():
     return 1100.0, "nominal dense TF32"
 
 
+def ncu_tf32_peak_tflops():
+    """The TF32 tensor peak ncu reports for this part
+    (sm__ops_path_tensor_op_utchmma_src_tf32_dst_fp32_sparsity_off ... peak_sustained_elapsed,
+    in ops/ns) in the committed k_contract_tc summary; None when absent."""
+    p = os.path.join(ROOT, "profiles", "k_contract_tc_dense15.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if "peak_sustained_elapsed.per_second" in line and "tf32" in line:
+            cells = [c.strip() for c in line.split("|")]
+            try:
+                return float(cells[2].replace(",", "")) * 1e9 / 1e12
+            except (ValueError, IndexError):
+                return None
+    return None
+
+
 def fp32_peak_tflops():
     """Nominal FP32 (non-tensor) peak: 148 SMs x 128 lanes x 2 flops x max SM clock.
     MEASURED_PEAKS.json carries no FP32 figure."""
@@ -453,6 +470,7 @@ def ours_arm(args, dist):
     if args.profile_only:
         print(json.dumps({"kernels_chosen": chosen}))
         batch.propagate(R)
+        batch.result(0)  # getResult (k_result) once
         return None
     # per-kernel device times (un-graphed, one event pair per launch)
     prof = batch.profile(2)
@@ -560,9 +578,13 @@ def ours_arm(args, dist):
         useful = 8.0 * probe.n_modes ** 4 * probe.nt * args.batch
         t = kc["ms_per_launch"] / 1e3
         t_tensor = tflops / (tpeak * 1e12)
+        npeak = ncu_tf32_peak_tflops()
         kc.update({"tensor_flops_per_launch": tflops, "achieved_tensor_tflops": tflops / t / 1e12,
                    "tensor_frac": tflops / t / 1e12 / tpeak,
+                   "ncu_tf32_peak_tflops": npeak,
+                   "tensor_frac_of_ncu_tf32_peak": (tflops / t / 1e12 / npeak) if npeak else None,
                    "useful_gemm_flops_per_launch": useful, "useful_gemm_tflops": useful / t / 1e12,
+                   "useful_gemm_frac_of_measured_bf16_burst": useful / t / 1e12 / (2 * tpeak),
                    "roofline_bound": "tensor" if t_tensor >= kc["alg_bytes_per_launch"] / (peak * 1e9) else "hbm",
                    "roofline_frac": max(t_tensor, kc["alg_bytes_per_launch"] / (peak * 1e9)) / t})
     traffic_solve = read_ncu_traffic(names[dom].split("+")[0], args.workload)
@@ -570,7 +592,11 @@ def ours_arm(args, dist):
     if tc and dom == "contract":
         roof = {"bound": "tensor", "kernel": names[dom], "achieved": kd["achieved_tensor_tflops"], "peak": tpeak,
                 "unit": "TFLOP/s", "frac": kd["tensor_frac"], "peak_source": tpeak_src,
-                "tensor_flops_per_launch": kd["tensor_flops_per_launch"]}
+                "tensor_flops_per_launch": kd["tensor_flops_per_launch"],
+                "note": "achieved counts the issued TF32 MMA work (3 split products per product); "
+                        "frac_of_ncu_tf32_peak and useful_gemm_tflops (8 M^4 NT per stage and solve) beside it",
+                "frac_of_ncu_tf32_peak": kd["tensor_frac_of_ncu_tf32_peak"],
+                "useful_gemm_tflops": kd["useful_gemm_tflops"]}
     elif kd["roofline_bound"] == "fp32":
         roof = {"bound": "fp32", "kernel": names[dom], "achieved": kd["achieved_tflops"], "peak": fpeak,
                 "unit": "TFLOP/s", "frac": kd["fp32_frac"],
