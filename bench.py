@@ -271,19 +271,27 @@ def stage_bytes(prob, tab_s, a, b, bt, pairs, raman_path):
     return {"pair": pair, "contract": contract, "nu": nu / tab_s}
 
 
-def stage_flops(prob, pairs, n_terms, raman_path):
-    """Algorithmic FP32 flops per launch for each kernel kind, one solve: 5 N log2 N per
-    complex transform; the recurrence 24 flops per sample and pair field (two complex
-    first-order scans, output and pair product); 8 per contraction term and sample;
-    about 70 per sample for k_nu's phase factors and stage combination."""
+def stage_flops(prob, pairs, n_terms, raman_path, recurrence_in_contract=False):
+    """Algorithmic FP32 flops per launch for each kernel kind, one solve, on the
+    per-sample model of the hot path: 5 N log2 N per complex transform; the Raman
+    recurrence 24 flops per sample and pair field (pair product, two complex first-order
+    steps, output); the contraction 6 per pair field (pair products) plus 8 per non-zero
+    term for the Kerr part and 8 more for the Raman part (NT (6 P + 8 nnz (1 + r)));
+    about 70 per sample for k_nu's phase factors and stage combination. When the
+    contraction kernel runs the recurrence through its own tiles (k_contract, k_contract_sr)
+    the recurrence's flops are its own; the pair kernel then only forms the tile
+    aggregates (the same 24 per sample and pair field)."""
     M, NT = prob.n_modes, prob.nt
     P = pairs if prob.raman else 0
+    r = 1 if prob.raman else 0
     fft = 5.0 * NT * math.log2(NT)
     if raman_path == 0:
         pair = P * (2 * fft + 12 * NT)
     else:
         pair = P * NT * 24.0
-    contract = NT * (8.0 * n_terms + 6.0 * P)
+    contract = NT * (8.0 * n_terms * (1 + r) + 6.0 * pairs)
+    if recurrence_in_contract:
+        contract += P * NT * 24.0
     nu = M * (2 * fft + 70.0 * NT)
     return {"pair": pair, "contract": contract, "nu": nu}
 
@@ -543,10 +551,10 @@ def ours_arm(args, dist):
     raman_path = info["raman_recurrence"]
     n_terms = int((probe.coupling["value"] != 0).sum())
     per = stage_bytes(probe, tab[3], tab[0], tab[1], bt, n_pairs, raman_path)
-    flops = stage_flops(probe, n_pairs, n_terms, raman_path)
     tc = bool(info.get("tensor_core_contraction", 0))
     pc = bool(info.get("contract_pair_chunk", 0))
     sr = bool(info.get("contract_sub_block", 0))
+    flops = stage_flops(probe, n_pairs, n_terms, raman_path, recurrence_in_contract=(raman_path == 2))
     names = {"pair": ("k_pair", "k_raman_scan", "k_raman_agg+k_raman_carry")[raman_path],
              "contract": ("k_contract_tc" if tc else "k_contract_sr" if sr else "k_contract_pc" if pc
                           else "k_contract"), "nu": "k_nu"}

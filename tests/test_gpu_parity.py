@@ -343,6 +343,18 @@ def test_serial_recurrence_contraction_against_oracle(mmp, monkeypatch, raman, o
         assert mo.rel_l2_per_mode(out, out_o).max() < (2e-6 if fl == 0 else 1e-12)
 
 
+@pytest.mark.parametrize("seed,M,nnz", [(170, 36, 1500), (172, 40, 1000)])
+def test_serial_recurrence_beyond_32_modes(mmp, seed, M, nnz):
+    # more than 32 modes: two rounds of the phase-B plan and two staged U items per thread
+    # (M * 8 sample pairs > 256 threads); 313 / 241 pair fields
+    prob = _tall_case(seed, True, M=M, nnz=nnz)
+    ref = mo.solve(prob)
+    for fl, tol in ((0, TOL32), (capi.MMP_F_FP64, TOL64)):
+        out, info = run(mmp, prob, [prob.n_steps], fl)
+        assert info["contract_sub_block"] == 16 and info["n_modes"] == M, info
+        assert mo.rel_l2_per_mode(out, ref).max() < tol
+
+
 def test_serial_recurrence_batch_members_match_single_solves(mmp, pinned):
     # members of different M and coupling in one batch, each a tall tile on its own too
     # (so its single solve runs the same kernel): each CTA reads its own solve's merged
