@@ -281,6 +281,7 @@ void worker_loop(mmp_server* sv) {
         continue;
       }
       if (e != cudaSuccess) set_fatal(sv, fail(MMP_ECUDA, cudaGetErrorString(e)));
+      mmp_detail::Range range("mmp.server.complete");
       complete(sv, (int)pi, K);
       progressed = true;
     }
@@ -295,11 +296,15 @@ void worker_loop(mmp_server* sv) {
         continue;
       }
     }
-    progressed |= admit_waiting(sv);
+    {
+      mmp_detail::Range range("mmp.server.admit");
+      progressed |= admit_waiting(sv);
+    }
     // launch
     for (auto& pl : sv->pools) {
       if (pl.in_flight || pl.used == 0) continue;
       mmp_batch* b = pl.b;
+      mmp_detail::Range range("mmp.server.launch");
       int rc = build_graph(b, K);
       if (rc == MMP_OK) {
         cudaError_t e = cudaGraphLaunch(b->graph, b->stream);

@@ -17,6 +17,10 @@
 #include <string>
 #include <vector>
 
+#ifndef MMP_NO_NVTX
+#include <nvtx3/nvToolsExt.h>
+#endif
+
 #include "kernel_table.h"
 #include "mmp.h"
 #include "stage_kernels.cuh"
@@ -85,6 +89,19 @@ int fail(int code, const std::string& msg) { return fail_c(code, msg.c_str()); }
 }  // namespace
 
 namespace mmp_detail {
+// NVTX range over a host-side phase (create, autotune, propagate, result, ...), for
+// timeline tools: a push and a pop of a named range, no-ops unless a tool is attached.
+// Build with -DMMP_NO_NVTX to leave them out.
+struct Range {
+#ifndef MMP_NO_NVTX
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+#else
+  explicit Range(const char*) {}
+#endif
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 // for the other units (io.cpp, noalloc.cu): record the text mmp_last_error returns
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 int set_error_c(int code, const char* msg) { return fail_c(code, msg); }
@@ -853,6 +870,7 @@ int capture_steps(mmp_batch* b, int steps) {
 
 int build_graph(mmp_batch* b, int steps) {
   if (b->graph && b->graph_steps == steps) return MMP_OK;
+  mmp_detail::Range range("mmp.capture_graph");
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -893,6 +911,7 @@ int check_status(mmp_batch* b) {
 
 int batch_propagate_async(mmp_batch* b, uint32_t nz) {
   if (!b) return fail(MMP_EINVAL, "NULL batch");
+  mmp_detail::Range range("mmp.propagate");
   CUDA_TRY(cudaSetDevice(b->device));
   for (auto& s : b->members) {
     if (!s.block) continue;  // empty slot
@@ -934,6 +953,7 @@ int batch_propagate_async(mmp_batch* b, uint32_t nz) {
 }
 
 int batch_sync(mmp_batch* b) {
+  mmp_detail::Range range("mmp.synchronize");
   CUDA_TRY(cudaSetDevice(b->device));
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   return check_status(b);
@@ -941,6 +961,7 @@ int batch_sync(mmp_batch* b) {
 
 int member_result(mmp_batch* b, uint32_t idx, double* out) {
   if (!b || idx >= b->members.size() || !out) return fail(MMP_EINVAL, "bad result arguments");
+  mmp_detail::Range range("mmp.get_result");
   CUDA_TRY(cudaSetDevice(b->device));
   Member& s = b->members[idx];
   int rc = launch_row_kernel(b, b->ks64, b->ks64.result, (int)s.M, 1, 0, b->d_descs + idx);
@@ -953,6 +974,7 @@ int member_result(mmp_batch* b, uint32_t idx, double* out) {
 
 int member_set_fields(mmp_batch* b, uint32_t idx, const double* phi0) {
   if (!b || idx >= b->members.size() || !phi0) return fail(MMP_EINVAL, "bad set_fields arguments");
+  mmp_detail::Range range("mmp.set_fields");
   CUDA_TRY(cudaSetDevice(b->device));
   Member& s = b->members[idx];
   for (size_t t = 0; t < 2 * (size_t)s.M * s.nt; ++t)
@@ -1534,6 +1556,7 @@ int restore_members(mmp_batch* b, const mmp_params* const* params) {
 }
 
 int autotune(mmp_batch* b, const mmp_params* const* params) {
+  mmp_detail::Range range("mmp.autotune");
   const KernelSet base = kernels_for(b->fp64 ? 1 : 0, b->logn, 0);
   const KernelSet alt = kernels_for(b->fp64 ? 1 : 0, b->logn, 1);
   std::vector<int> xcs = {0}, tiles = tile_candidates(b), gs = {1};
@@ -1617,6 +1640,7 @@ int create_batch(const mmp_params* const* params, uint32_t n, mmp_batch** out) {
   if (!out) return fail(MMP_EINVAL, "out is NULL");
   *out = nullptr;
   if (!params || n == 0) return fail(MMP_EINVAL, "empty batch");
+  mmp_detail::Range range("mmp.create");
   for (uint32_t i = 0; i < n; ++i) {
     std::string why;
     int rc = validate(params[i], why);
@@ -1763,6 +1787,7 @@ int mmp_batch_propagate_timed(mmp_batch* b, uint32_t nz, uint32_t repeats, doubl
 
 int mmp_batch_profile(mmp_batch* b, uint32_t nz, double* ms_per_launch, uint32_t* launches) {
   if (!b || !ms_per_launch || !launches) return fail(MMP_EINVAL, "bad profile arguments");
+  mmp_detail::Range range("mmp.profile");
   CUDA_TRY(cudaSetDevice(b->device));
   for (int k = 0; k < 3; ++k) { ms_per_launch[k] = 0.0; launches[k] = 0; }
   for (auto& s : b->members) {
@@ -1876,6 +1901,7 @@ int mmp_propagate_snapshots(mmp_solver* sol, uint32_t n_save, int z_mode, double
                             double* elapsed_s) {
   if (!sol) return fail(MMP_EINVAL, "NULL solver");
   if (n_save == 0) return fail(MMP_EINVAL, "n_save must be >= 1");
+  mmp_detail::Range range("mmp.snapshots");
   if (z_mode != 0 && z_mode != 1) return fail(MMP_EINVAL, "z_mode must be 0 (continuous) or 1 (reference)");
   const auto t0 = std::chrono::steady_clock::now();
   mmp_batch* b = sol->b;
@@ -1966,6 +1992,7 @@ int mmp_tableau(uint32_t method_order, int32_t rk_variant, double rk_lambda, dou
 int mmp_dft(uint32_t n, uint32_t rows, int direction, int fp64, const double* in, double* out) {
   if (!in || !out || rows == 0) return fail(MMP_EINVAL, "bad dft arguments");
   if (direction != -1 && direction != 1) return fail(MMP_EINVAL, "direction must be -1 or +1");
+  mmp_detail::Range range("mmp.dft");
   const int lg = ilog2_exact(n);
   if (lg < kMinLogN || lg > kMaxLogN) return fail(MMP_ENOTSUP, "n must be a power of two in [64, 65536]");
   int dev = 0;
