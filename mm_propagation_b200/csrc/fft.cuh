@@ -3,11 +3,16 @@
 //
 // Row of N = 2^LOGN complex samples in precision T (float or double).
 //  * C = 2^LOGC CTAs (a cluster) share a row when N * sizeof(T2) > 128 KB.
-//    CTA c holds the decimated sub-sequence x[c + C*u], u < NL = N / C, in its
-//    shared memory and transforms it locally; a radix-C butterfly across the
-//    cluster, reading and writing peer CTAs' shared memory (DSMEM), combines
-//    the C local spectra (decimation in time). The inverse runs the same steps
-//    backwards (split across the cluster, then local inverse transforms).
+//    The row is cut into runs of G consecutive samples, G * sizeof(T2) = 32 bytes (one
+//    DRAM sector: G = 4 in FP32, 2 in FP64), dealt out to the CTAs in turn: CTA r holds
+//    the samples t = g + G (r + C v), g < G, v < NL/G (NL = N / C), so that its global
+//    loads and stores move whole sectors. In shared memory they are G rows of NL/G:
+//    row g is the sub-sequence x_g[s] = x[g + G s] at s = r + C v, decimated over the
+//    cluster. Forward: every CTA transforms its G rows locally (NL/G points each); a
+//    radix-(C G) butterfly combines, per frequency, the partial spectra of the G rows
+//    of all C CTAs, read through distributed shared memory (decimation in time over
+//    the C G sub-sequences x[n + C G u]). The inverse runs the same steps backwards.
+//    With C = 1, G = 1 and the row is one local transform.
 //  * The local transform is an in-place Stockham autosort FFT in padded
 //    shared memory: each thread keeps E = 2^LOGE samples in registers per pass,
 //    runs radix-2^r butterflies on them, and writes them back in Stockham order,
@@ -15,10 +20,10 @@
 //  * Twiddles come from per-size tables w_n[m] = exp(-2 pi i m / n), computed in
 //    FP64 on the host and rounded to T.
 //
-// Frequency-domain samples are handed between the FFT and the kernels'
-// point-wise math in registers: register slot i of a thread holds frequency
-// freq_index(i) (see Geo). Time-domain samples stay in shared memory: local
-// index u holds time t = rank + C*u.
+// Frequency-domain samples stay in shared memory in the "combined layout" (Geo::freq_of:
+// C G spans of CH consecutive frequencies per CTA). Time-domain samples: local row g,
+// column v holds time g + G (rank + C v); kernels walk them in time order with
+// Geo::time_of_w / Geo::local_of_w, so that a warp's accesses cover whole sectors.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -142,16 +147,26 @@ template <int R, bool INV> struct RegDFT {
 
 
 // Twiddle tables: tw.f[L] / tw.d[L] point at 2^L entries exp(-2 pi i m / 2^L).
+// cf[L][xc] / cd[L][xc]: the cluster combine's twiddles of a split row of 2^L samples
+// (row split xc), [n][kl] = exp(-2 pi i n kl / 2^L) for n < CG, kl < 2^L / CG (CG = C G of
+// that geometry), so that a warp's lanes (consecutive kl) read consecutive entries; null
+// where not built (the combine then reads the 2^L table at n kl).
 struct TwTables {
   const float2* f[17];
   const double2* d[17];
+  const float2* cf[17][2];
+  const double2* cd[17][2];
 };
 template <typename T> __device__ __forceinline__ const c2<T>* tw_table(const TwTables& t, int L);
 template <> __device__ __forceinline__ const float2* tw_table<float>(const TwTables& t, int L) { return t.f[L]; }
 template <> __device__ __forceinline__ const double2* tw_table<double>(const TwTables& t, int L) { return t.d[L]; }
+template <typename T> __device__ __forceinline__ const c2<T>* cmb_table(const TwTables& t, int L, int xc);
+template <> __device__ __forceinline__ const float2* cmb_table<float>(const TwTables& t, int L, int xc) { return t.cf[L][xc]; }
+template <> __device__ __forceinline__ const double2* cmb_table<double>(const TwTables& t, int L, int xc) { return t.cd[L][xc]; }
 
 // Geometry of one row transform.
 template <typename T, int LOGN_, int XC_ = 0> struct Geo {
+  using Real = T;
   static constexpr int LOGN = LOGN_;
   static constexpr int N = 1 << LOGN;
   static constexpr int LOGSZ = sizeof(c2<T>) == 8 ? 3 : 4;
@@ -159,32 +174,50 @@ template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   static constexpr int C = 1 << LOGC;
   static constexpr int LOGL = LOGN - LOGC;
   static constexpr int NL = 1 << LOGL;
+  // runs of G samples (32 bytes) per CTA on split rows; G rows of NLG in shared memory
+  static constexpr int LOGG = LOGC > 0 ? 5 - LOGSZ : 0;
+  static constexpr int G = 1 << LOGG;
+  static constexpr int LOGNLG = LOGL - LOGG;
+  static constexpr int NLG = 1 << LOGNLG;
   static constexpr int LOGE_PREF = (sizeof(T) == 4 && LOGL >= 13) ? 5 : 4;
   static constexpr int LOGE_CAP = LOGL - 5 > 1 ? LOGL - 5 : 1;  // keep >= 32 threads
   static constexpr int LOGE = LOGE_PREF < LOGE_CAP ? LOGE_PREF : LOGE_CAP;
   static constexpr int E = 1 << LOGE;
   static constexpr int NTHR = NL / E;
-  static constexpr int LOGCH = LOGL - LOGC;
-  static constexpr int CH = NL / C;       // frequencies k a CTA combines
-  static constexpr int LOGQ = LOGL - 2;   // quarter-wave twiddle table: NL/4 entries
-  static constexpr int DATA_BYTES = padded_len(NL) * (int)sizeof(c2<T>);
-  static constexpr int TWQ_BYTES = padded_len(NL / 4) * (int)sizeof(c2<T>);
+  static constexpr int LOGCH = LOGNLG - LOGC;
+  static constexpr int CH = 1 << LOGCH;  // frequencies per span: C G spans per CTA
+  static constexpr int LOGQ = LOGNLG - 2;  // quarter-wave twiddle table of the local size
+  // rows g > 0 start SKEW elements later (mod 128 bytes), so that a warp walking the
+  // samples in time order (row g = lane mod G) reads and writes without bank conflicts
+  static constexpr int SKEW = LOGG > 0 ? 4 : 0;
+  static constexpr int DATA_BYTES = (padded_len(NL) + (G - 1) * SKEW) * (int)sizeof(c2<T>);
+  static constexpr int TWQ_BYTES = padded_len(NLG / 4) * (int)sizeof(c2<T>);
   static constexpr int SMEM_BYTES = DATA_BYTES + TWQ_BYTES;
   // split rows (XC_ > 0) are sized so that two CTAs share an SM
   static constexpr int MIN_BLOCKS = (XC_ > 0 && SMEM_BYTES <= 110 * 1024 && NTHR <= 512) ? 2 : 1;
-  static_assert(LOGE >= LOGC, "each thread must combine at least one frequency per CTA");
+  static_assert(LOGE >= LOGC + LOGG, "each thread must combine at least one frequency per CTA");
+  static_assert(LOGNLG - LOGE >= 5 || LOGG == 0, "a warp's butterflies stay within one row");
   static_assert(NTHR >= 32 && NTHR <= 1024, "block size");
   static_assert(DATA_BYTES % 16 == 0, "twiddle table alignment");
 
+  // shared-memory offset of local index i (row i >> LOGNLG)
+  __host__ __device__ __forceinline__ static int sidx(int i) { return pad(i) + (i >> LOGNLG) * SKEW; }
   // Spectrum layout in shared memory after a forward transform ("combined layout"):
-  // local index i holds frequency rank*CH + (i mod CH) + NL*(i div CH); for C = 1
+  // local index i holds frequency rank*CH + (i mod CH) + NLG*(i div CH); for C = 1
   // that is just i.
   __device__ __forceinline__ static int freq_of(int rank, int i) {
     if constexpr (C == 1) return i;
-    else return rank * CH + (i & (CH - 1)) + NL * (i >> LOGCH);
+    else return rank * CH + (i & (CH - 1)) + NLG * (i >> LOGCH);
   }
-  // Time layout: local index u holds time rank + C*u.
-  __device__ __forceinline__ static int time_of(int rank, int u) { return rank + C * u; }
+  // The CTA's time samples in time order, w < NL: time and local index of the w-th.
+  __device__ __forceinline__ static int time_of_w(int rank, int w) {
+    if constexpr (C == 1) return w;
+    else return ((((w >> LOGG) << LOGC) + rank) << LOGG) + (w & (G - 1));
+  }
+  __device__ __forceinline__ static int local_of_w(int w) {
+    if constexpr (C == 1) return w;
+    else return ((w & (G - 1)) << LOGNLG) + (w >> LOGG);
+  }
 };
 
 // exp(-2 pi i m / NL) (conjugated for INV) from the quarter-wave table
@@ -203,146 +236,189 @@ __device__ __forceinline__ V tw_quarter(const V* __restrict__ sq, int m) {
   return r;
 }
 
-// Copy the first quarter of the size-NL table into shared memory.
+// Copy the first quarter of the local transform's table (NLG points) into shared memory.
 template <typename T, int LOGN, int XC>
 __device__ __forceinline__ c2<T>* load_twiddles(unsigned char* smem_raw, const TwTables& tw) {
   using Gm = Geo<T, LOGN, XC>;
   c2<T>* sq = reinterpret_cast<c2<T>*>(smem_raw + Gm::DATA_BYTES);
-  const c2<T>* g = tw_table<T>(tw, Gm::LOGL);
+  const c2<T>* g = tw_table<T>(tw, Gm::LOGNLG);
 #pragma unroll 4
-  for (int m = threadIdx.x; m < Gm::NL / 4; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
+  for (int m = threadIdx.x; m < Gm::NLG / 4; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
   return sq;
 }
 
-// One in-place Stockham pass of radix 2^LOGR at stride Ns = 2^logns (runtime).
-template <typename T, int LOGL, int LOGE, int LOGR, bool INV>
-__device__ __forceinline__ void stockham_pass(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, int logns) {
-  using V = c2<T>;
-  constexpr int NL = 1 << LOGL, E = 1 << LOGE, NTHR = NL / E;
-  constexpr int R = 1 << LOGR, NB = E / R, LOGQ = LOGL - 2;
+// One in-place Stockham pass of radix 2^LOGR at stride Ns = 2^logns (runtime) over the
+// rows of Gm (G rows of NLG samples; a thread's butterflies j < NL/R, row j / (NLG/R)).
+template <typename Gm, int LOGR, bool INV>
+__device__ __forceinline__ void stockham_pass(c2<typename Gm::Real>* __restrict__ s,
+                                              const c2<typename Gm::Real>* __restrict__ sq, int logns) {
+  using V = c2<typename Gm::Real>;
+  constexpr int LOGB = Gm::LOGNLG;  // row length
+  constexpr int NB = 1 << LOGB, E = Gm::E, NTHR = Gm::NTHR;
+  constexpr int R = 1 << LOGR, NBF = E / R;
+  constexpr int LOGJ = LOGB - LOGR;  // butterflies per row
   const int tid = threadIdx.x;
   V v[E];
 #pragma unroll
-  for (int bf = 0; bf < NB; ++bf) {
-    const int j = tid + bf * NTHR;
+  for (int bf = 0; bf < NBF; ++bf) {
+    const int ja = tid + bf * NTHR;
+    const int base = (ja >> LOGJ) << LOGB, j = ja & ((1 << LOGJ) - 1);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[bf * R + r] = s[pad(j + r * (NL / R))];
+    for (int r = 0; r < R; ++r) v[bf * R + r] = s[Gm::sidx(base + j + r * (NB / R))];
   }
   __syncthreads();
   const int nsm = (1 << logns) - 1;
 #pragma unroll
-  for (int bf = 0; bf < NB; ++bf) {
-    const int j = tid + bf * NTHR;
+  for (int bf = 0; bf < NBF; ++bf) {
+    const int ja = tid + bf * NTHR;
+    const int base = (ja >> LOGJ) << LOGB, j = ja & ((1 << LOGJ) - 1);
     const int jm = j & nsm;
     if (logns > 0) {
-      const int step = jm << (LOGL - logns - LOGR);  // jm * NL / (Ns * R)
+      const int step = jm << (LOGB - logns - LOGR);  // jm * NB / (Ns * R)
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_quarter<V, INV, LOGQ>(sq, r * step));
+      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_quarter<V, INV, Gm::LOGQ>(sq, r * step));
     }
     RegDFT<R, INV>::run(&v[bf * R]);
     const int idxD = ((j >> logns) << (logns + LOGR)) + jm;
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[pad(idxD + (r << logns))] = v[bf * R + r];
+    for (int r = 0; r < R; ++r) s[Gm::sidx(base + idxD + (r << logns))] = v[bf * R + r];
   }
   __syncthreads();
 }
 
-// Local transform of the NL samples in shared memory (natural order in and out,
-// unnormalised). One pass body per radix keeps the instruction footprint small.
+// Local transform of the G rows of NLG samples in shared memory (natural order in and
+// out, unnormalised). One pass body per radix keeps the instruction footprint small.
 template <typename T, int LOGN, int XC, bool INV>
 __device__ __noinline__ void local_fft(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq) {
   using Gm = Geo<T, LOGN, XC>;
-  constexpr int FULL = Gm::LOGL / Gm::LOGE, REM = Gm::LOGL % Gm::LOGE;
+  constexpr int FULL = Gm::LOGNLG / Gm::LOGE, REM = Gm::LOGNLG % Gm::LOGE;
   __syncthreads();
   int logns = 0;
 #pragma unroll 1
   for (int p = 0; p < FULL; ++p) {
-    stockham_pass<T, Gm::LOGL, Gm::LOGE, Gm::LOGE, INV>(s, sq, logns);
+    stockham_pass<Gm, Gm::LOGE, INV>(s, sq, logns);
     logns += Gm::LOGE;
   }
-  if constexpr (REM > 0) stockham_pass<T, Gm::LOGL, Gm::LOGE, REM, INV>(s, sq, logns);
+  if constexpr (REM > 0) stockham_pass<Gm, REM, INV>(s, sq, logns);
 }
 
-// Forward transform of the time samples in shared memory (local u = time rank + C*u);
-// leaves the spectrum in shared memory in the combined layout (Geo::freq_of).
+// w[n] = w_N^{n kl}, 0 < n < CG: row n of the combine table at kl, or the N-point table
+// at n kl where no combine table is given.
+template <typename Gm>
+__device__ __forceinline__ void combine_twiddles(c2<typename Gm::Real>* w, const c2<typename Gm::Real>* twc,
+                                                 const c2<typename Gm::Real>* twN, int kl) {
+  constexpr int CG = Gm::C * Gm::G;
+  if (twc) {
+#pragma unroll
+    for (int n = 1; n < CG; ++n) w[n] = __ldg(&twc[n * Gm::NLG + kl]);
+  } else {
+#pragma unroll
+    for (int n = 1; n < CG; ++n) w[n] = __ldg(&twN[n * kl]);
+  }
+}
+
+// Forward transform of the time samples in shared memory (row g, column v: time
+// g + G (rank + C v)); leaves the spectrum in shared memory in the combined layout
+// (Geo::freq_of). Row g of CTA c is the sub-sequence x[n + CG u], n = g + G c, u < NLG
+// (CG = C G), so with F_n its local NLG-point spectrum (decimation in time):
+//   X[kl + NLG j] = sum_n w_CG^{n j} w_N^{n kl} F_n[kl],  kl < NLG, j < CG.
+// A thread handles K = E / CG values kl = rank CH + i, i = tid + jj NTHR: CG inputs each
+// (G rows in each of the C CTAs), one radix-CG DFT, CG outputs, all of them frequencies
+// this CTA keeps (span j, offset i). Every remote read is issued before the cluster
+// barrier that lets the CTAs overwrite their rows. Out of line: its registers are its own.
 template <typename T, int LOGN, int XC>
-__device__ __forceinline__ void forward(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
+__device__ __noinline__ void combine_fwd(c2<T>* __restrict__ s, const TwTables& tw) {
   using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
-  local_fft<T, LOGN, XC, false>(s, sq);
   if constexpr (Gm::C > 1) {
+    constexpr int C = Gm::C, G = Gm::G, CG = C * G, K = Gm::E / CG;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int tid = threadIdx.x;
     const V* twN = tw_table<T>(tw, Gm::LOGN);
-    V out[Gm::E];
-    cl.sync();  // every CTA finished its local transform
+    V v[K][CG];
+    cl.sync();  // every CTA finished its local transforms
 #pragma unroll
-    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
-      const int k = rank * Gm::CH + tid + jj * Gm::NTHR;
-      V vals[Gm::C];
+    for (int c = 0; c < C; ++c) {
+      const V* peer = cl.map_shared_rank(s, c);
 #pragma unroll
-      for (int c = 0; c < Gm::C; ++c) {
-        const V* peer = cl.map_shared_rank(s, c);
-        V f = peer[pad(k)];
-        if (c > 0) f = cmul(f, __ldg(&twN[c * k]));
-        vals[c] = f;
+      for (int jj = 0; jj < K; ++jj) {
+        const int kl = rank * Gm::CH + tid + jj * Gm::NTHR;
+#pragma unroll
+        for (int g = 0; g < G; ++g) v[jj][g + G * c] = peer[Gm::sidx(g * Gm::NLG + kl)];
       }
-      RegDFT<Gm::C, false>::run(vals);
+    }
+    const V* twc = cmb_table<T>(tw, Gm::LOGN, XC);
 #pragma unroll
-      for (int q = 0; q < Gm::C; ++q) out[jj * Gm::C + q] = vals[q];
+    for (int jj = 0; jj < K; ++jj) {
+      const int kl = rank * Gm::CH + tid + jj * Gm::NTHR;
+      V w[CG];
+      combine_twiddles<Gm>(w, twc, twN, kl);
+#pragma unroll
+      for (int n = 1; n < CG; ++n) v[jj][n] = cmul(v[jj][n], w[n]);
+      RegDFT<CG, false>::run(v[jj]);
     }
     cl.sync();  // all peer reads done before shared memory is overwritten
 #pragma unroll
-    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
-      const int kl = tid + jj * Gm::NTHR;
+    for (int jj = 0; jj < K; ++jj) {
+      const int i = tid + jj * Gm::NTHR;
 #pragma unroll
-      for (int q = 0; q < Gm::C; ++q) s[pad(kl + Gm::CH * q)] = out[jj * Gm::C + q];
+      for (int j = 0; j < CG; ++j) s[Gm::sidx(j * Gm::CH + i)] = v[jj][j];
     }
     __syncthreads();
   }
 }
+template <typename T, int LOGN, int XC>
+__device__ __forceinline__ void forward(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
+  local_fft<T, LOGN, XC, false>(s, sq);
+  if constexpr (Geo<T, LOGN, XC>::C > 1) combine_fwd<T, LOGN, XC>(s, tw);
+}
 
 // Inverse transform of a spectrum in shared memory in the combined layout; leaves
-// the (unnormalised) time samples in shared memory, local u = time rank + C*u.
+// the (unnormalised) time samples in shared memory (row g, column v: time
+// g + G (rank + C v)): the forward steps backwards with conjugate twiddles.
 template <typename T, int LOGN, int XC>
-__device__ __forceinline__ void inverse(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
+__device__ __noinline__ void combine_inv(c2<T>* __restrict__ s, const TwTables& tw) {
   using Gm = Geo<T, LOGN, XC>;
   using V = c2<T>;
   if constexpr (Gm::C > 1) {
+    constexpr int C = Gm::C, G = Gm::G, CG = C * G, K = Gm::E / CG;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int tid = threadIdx.x;
     const V* twN = tw_table<T>(tw, Gm::LOGN);
-    V out[Gm::E];
+    V v[K][CG];
     __syncthreads();  // the caller's writes of the spectrum are complete
+    const V* twc = cmb_table<T>(tw, Gm::LOGN, XC);
 #pragma unroll
-    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
-      const int kl = tid + jj * Gm::NTHR;
-      const int k = rank * Gm::CH + kl;
-      V vals[Gm::C];
+    for (int jj = 0; jj < K; ++jj) {
+      const int i = tid + jj * Gm::NTHR;
+      const int kl = rank * Gm::CH + i;
 #pragma unroll
-      for (int q = 0; q < Gm::C; ++q) vals[q] = s[pad(kl + Gm::CH * q)];
-      RegDFT<Gm::C, true>::run(vals);
+      for (int j = 0; j < CG; ++j) v[jj][j] = s[Gm::sidx(j * Gm::CH + i)];
+      RegDFT<CG, true>::run(v[jj]);
+      V w[CG];
+      combine_twiddles<Gm>(w, twc, twN, kl);
 #pragma unroll
-      for (int c = 0; c < Gm::C; ++c) {
-        V f = vals[c];
-        if (c > 0) f = cmulc(f, __ldg(&twN[c * k]));
-        out[jj * Gm::C + c] = f;
-      }
+      for (int n = 1; n < CG; ++n) v[jj][n] = cmulc(v[jj][n], w[n]);
     }
     cl.sync();  // every CTA is running and has read its own spectrum
 #pragma unroll
-    for (int jj = 0; jj < Gm::E / Gm::C; ++jj) {
-      const int k = rank * Gm::CH + tid + jj * Gm::NTHR;
+    for (int c = 0; c < C; ++c) {
+      V* peer = cl.map_shared_rank(s, c);
 #pragma unroll
-      for (int c = 0; c < Gm::C; ++c) {
-        V* peer = cl.map_shared_rank(s, c);
-        peer[pad(k)] = out[jj * Gm::C + c];
+      for (int jj = 0; jj < K; ++jj) {
+        const int kl = rank * Gm::CH + tid + jj * Gm::NTHR;
+#pragma unroll
+        for (int g = 0; g < G; ++g) peer[Gm::sidx(g * Gm::NLG + kl)] = v[jj][g + G * c];
       }
     }
     cl.sync();  // all peer writes landed
   }
+}
+template <typename T, int LOGN, int XC>
+__device__ __forceinline__ void inverse(c2<T>* __restrict__ s, const c2<T>* __restrict__ sq, const TwTables& tw) {
+  if constexpr (Geo<T, LOGN, XC>::C > 1) combine_inv<T, LOGN, XC>(s, tw);
   local_fft<T, LOGN, XC, true>(s, sq);
 }
 

@@ -186,12 +186,40 @@ int ensure_device(int dev, DeviceRes** out) {
     }
     off += n;
   }
+  // the split rows' combine tables, [n][kl] = w_L[n kl] (n < CG, kl < 2^L / CG), gathered
+  // from the tables above, so that they hold the same values
+  struct Cmb { int fp64, L, xc; size_t off; };
+  std::vector<Cmb> cm;
+  size_t cbytes = 0;
+  for (int fp64 = 0; fp64 < 2; ++fp64)
+    for (int L = kMinLogN; L <= kMaxLogN; ++L)
+      for (int xc = 0; xc < 2; ++xc) {
+        const KernelSet ks = kernels_for(fp64, L, xc);
+        if (!ks.prime || ks.C < 2) continue;
+        cm.push_back({fp64, L, xc, cbytes});
+        cbytes += ((size_t)1 << L) * (fp64 ? sizeof(double2) : sizeof(float2));
+      }
+  std::vector<unsigned char> hc(cbytes);
+  for (const Cmb& c : cm) {
+    const KernelSet ks = kernels_for(c.fp64, c.L, c.xc);
+    const size_t n = (size_t)1 << c.L;
+    const size_t CG = (size_t)ks.C * (c.fp64 ? 2 : 4);  // C times the run length G (32 bytes)
+    for (size_t kl = 0; kl < n / CG; ++kl)
+      for (size_t q = 0; q < CG; ++q) {
+        const size_t m = q * kl, e = q * (n / CG) + kl;
+        if (c.fp64) reinterpret_cast<double2*>(hc.data() + c.off)[e] = hd[offs[c.L] + m];
+        else reinterpret_cast<float2*>(hc.data() + c.off)[e] = hf[offs[c.L] + m];
+      }
+  }
+  // one allocation: FP64 tables | FP32 tables | combine tables
   void* mem = nullptr;
-  CUDA_TRY(dev_malloc(&mem, n_tot * (sizeof(double2) + sizeof(float2))));
+  CUDA_TRY(dev_malloc(&mem, n_tot * (sizeof(double2) + sizeof(float2)) + cbytes));
   double2* dd = (double2*)mem;
   float2* df = (float2*)(dd + n_tot);
+  unsigned char* dc = (unsigned char*)(df + n_tot);
   cudaError_t ce = cudaMemcpy(dd, hd.data(), n_tot * sizeof(double2), cudaMemcpyHostToDevice);
   if (ce == cudaSuccess) ce = cudaMemcpy(df, hf.data(), n_tot * sizeof(float2), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess && cbytes) ce = cudaMemcpy(dc, hc.data(), cbytes, cudaMemcpyHostToDevice);
   if (ce != cudaSuccess) {
     dev_free(mem);
     return fail(MMP_ECUDA, std::string("twiddle upload: ") + cudaGetErrorString(ce));
@@ -199,6 +227,10 @@ int ensure_device(int dev, DeviceRes** out) {
   for (int L = 0; L <= kMaxLogN; ++L) {
     r.tw.d[L] = L ? dd + offs[L] : nullptr;
     r.tw.f[L] = L ? df + offs[L] : nullptr;
+  }
+  for (const Cmb& c : cm) {
+    if (c.fp64) r.tw.cd[c.L][c.xc] = (const double2*)(dc + c.off);
+    else r.tw.cf[c.L][c.xc] = (const float2*)(dc + c.off);
   }
   r.tw_mem = mem;
   // dynamic shared memory opt-in for every instantiated kernel

@@ -221,13 +221,13 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
       }
     }
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * zs;
-    s[pad(li)] = cmul(from_d2<T>(x), expi<T>(th));
+    s[Gm::sidx(li)] = cmul(from_d2<T>(x), expi<T>(th));
   }
   inverse<T, LOGN, XC>(s, sq, kp.tw);
   V* U = as_t2<T>(d.U);
   const T inv = (T)d.inv_nt;
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[row + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
+  for (int w = tid; w < Gm::NL; w += Gm::NTHR) U[row + Gm::time_of_w(rank, w)] = cscale(s[Gm::sidx(Gm::local_of_w(w))], inv);
 }
 
 // ---- k_pair: R_q = IFFT(FFT(V_q) * H), V_q = U_l conj(U_m) -------------------------------
@@ -260,9 +260,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     }
   } else {
 #pragma unroll 8
-    for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
-      const int t = Gm::time_of(rank, u);
-      s[pad(u)] = cmulc(U[rl + t], U[rm + t]);
+    for (int w = tid; w < Gm::NL; w += Gm::NTHR) {
+      const int t = Gm::time_of_w(rank, w);
+      s[Gm::sidx(Gm::local_of_w(w))] = cmulc(U[rl + t], U[rm + t]);
     }
   }
   forward<T, LOGN, XC>(s, sq, kp.tw);
@@ -277,14 +277,14 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     }
   } else {
 #pragma unroll 4
-    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = cmul(s[pad(li)], __ldg(&H[Gm::freq_of(rank, li)]));
+    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[Gm::sidx(li)] = cmul(s[Gm::sidx(li)], __ldg(&H[Gm::freq_of(rank, li)]));
   }
   inverse<T, LOGN, XC>(s, sq, kp.tw);
   // R_q = (H_R conv V_q); the Kerr part (1 - fR) V_q is formed by the contraction from
   // the U tile it already holds
   V* R = as_t2<T>(d.W) + (size_t)q * Gm::N;
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) R[Gm::time_of(rank, u)] = s[pad(u)];
+  for (int w = tid; w < Gm::NL; w += Gm::NTHR) R[Gm::time_of_w(rank, w)] = s[Gm::sidx(Gm::local_of_w(w))];
 }
 
 // ---- k_raman_scan: R_q = h_R (*) V_q as a periodic linear recurrence ----------------------
@@ -519,13 +519,14 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // the descriptor and polynomial round trips below overlap the row's.
   V* sq = reinterpret_cast<V*>(smem_raw + Gm::DATA_BYTES);
   {
-    const c2<T>* g = tw_table<T>(kp.tw, Gm::LOGL);
-    for (int m = tid; m < Gm::NL / 4; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
+    const c2<T>* g = tw_table<T>(kp.tw, Gm::LOGNLG);
+    for (int m = tid; m < Gm::NLG / 4; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
     const SolveDesc* gd = kp.descs + blockIdx.y;
     if (p < __ldg(&gd->M)) {
       const V* sg = as_t2<T>(reinterpret_cast<const void*>(__ldg(reinterpret_cast<const unsigned long long*>(&gd->sigma)))) +
                     (size_t)p * Gm::N;
-      for (int u = tid; u < Gm::NL; u += Gm::NTHR) cp_async_c2<T>(&s[pad(u)], sg + Gm::time_of(rank, u));
+      for (int w = tid; w < Gm::NL; w += Gm::NTHR)
+        cp_async_c2<T>(&s[Gm::sidx(Gm::local_of_w(w))], sg + Gm::time_of_w(rank, w));
     }
     cp_async_commit();
   }
@@ -544,8 +545,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // Stage-combination list: the stored N_hat_j entering x_hat (or, at the last stage,
   // psi_{n+1} = psi_n + h sum_j b_j N_j, src/MultimodePropagation_CPU.cpp:75-85) with
   // their coefficients h*a or h*b; N_hat_i itself comes from registers (cself).
-  // Once its sigma loads are issued, thread 0 starts L2 prefetches of the psi_hat and
-  // N_hat_j spans this CTA reads after its forward transform, so they arrive while the
+  // Once the sigma loads are issued, the CTA's threads start L2 prefetches of the psi_hat
+  // and N_hat_j the cluster reads after its forward transform, so they arrive while the
   // transform runs.
   __shared__ int s_jq[kMaxStages];
   __shared__ double s_cq[kMaxStages];
@@ -573,14 +574,24 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     }
     s_nq = nq;
   }
-  if (tid == 0) {
-    const size_t prow = (size_t)p * Gm::N;
-    const size_t pstride = (size_t)d.M * Gm::N;
-    const V* Nq = as_t2<T>(d.Nh);
-    for (int qb = 0; qb < Gm::C; ++qb) {  // the CTA's frequencies: C spans of CH
-      const size_t f0 = prow + (size_t)rank * Gm::CH + (size_t)Gm::NL * qb;
-      prefetch_l2(d.psi_hat + f0, Gm::CH * (unsigned)sizeof(double2));
-      for (int q = 0; q < s_nq; ++q) prefetch_l2(Nq + (size_t)s_jq[q] * pstride + f0, Gm::CH * (unsigned)sizeof(V));
+  __syncthreads();  // s_jq, s_nq
+  {
+    // the row's psi_hat and N_hat_j, 1/C of each per CTA of the cluster (together the
+    // frequencies every CTA reads), one 32 KB piece per thread
+    constexpr unsigned kNBytes = Gm::NL * (unsigned)sizeof(V);
+    constexpr unsigned kPiece = kNBytes < 32u * 1024u ? kNBytes : 32u * 1024u;
+    constexpr unsigned kPsiPieces = (Gm::NL * (unsigned)sizeof(double2)) / kPiece;
+    constexpr unsigned kNPieces = kNBytes / kPiece;
+    const size_t f0 = (size_t)p * Gm::N + (size_t)rank * Gm::NL;
+    const unsigned np = kPsiPieces + (unsigned)s_nq * kNPieces;
+    for (unsigned t = tid; t < np; t += Gm::NTHR) {
+      if (t < kPsiPieces) {
+        prefetch_l2(d.psi_hat + f0 + (size_t)t * (kPiece / sizeof(double2)), kPiece);
+      } else {
+        const unsigned u = t - kPsiPieces, q = u / kNPieces, pc = u - q * kNPieces;
+        prefetch_l2(as_t2<T>(d.Nh) + (size_t)s_jq[q] * ((size_t)d.M * Gm::N) + f0 + (size_t)pc * (kPiece / sizeof(V)),
+                    kPiece);
+      }
     }
   }
   cp_async_wait<0>();                  // this thread's sigma and twiddle copies
@@ -629,7 +640,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         const int li = tid + (e0 + c) * Gm::NTHR;
         kk[c] = Gm::freq_of(rank, li);
         ps[c] = d.psi_hat[row + kk[c]];
-        sv[c] = s[pad(li)];
+        sv[c] = s[Gm::sidx(li)];
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
           if (q < nqr) nj[c][q] = Nh[(size_t)s_jq[q] * mstride + row + kk[c]];
@@ -709,7 +720,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         V en;
         if (same_z) en = ei;
         else en = expi<T>(L * znext);
-        s[pad(li)] = spec_in(cmul(xt, en));
+        s[Gm::sidx(li)] = spec_in(cmul(xt, en));
       }
     }
   };
@@ -731,7 +742,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     const double alpha = alpha_of(k, Gm::N, d.alpha_scale);
     const double L = im_L(poly, d.n_beta, alpha);
     // N_hat_i = i sgn(gamma) conj(E_i) FFT(sigma)   (src/MultimodePropagation_CPU.cpp:231-237)
-    const V xe = cmulc(s[pad(li)], expi<T>(L * zi));
+    const V xe = cmulc(s[Gm::sidx(li)], expi<T>(L * zi));
     V nh;
     nh.x = (T)(-d.sgn_gamma) * xe.y;
     nh.y = (T)(d.sgn_gamma) * xe.x;
@@ -763,7 +774,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         }
       }
     }
-    s[pad(li)] = spec_in(cmul(from_d2<T>(x), expi<T>(L * znext)));
+    s[Gm::sidx(li)] = spec_in(cmul(from_d2<T>(x), expi<T>(L * znext)));
   }
   }
   p_part += (double)p_part_f;
@@ -817,7 +828,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   } else {
     inverse<T, LOGN, XC>(s, sq, kp.tw);
 #pragma unroll 8
-    for (int u = tid; u < Gm::NL; u += Gm::NTHR) U[(size_t)p * Gm::N + Gm::time_of(rank, u)] = cscale(s[pad(u)], inv);
+    for (int w = tid; w < Gm::NL; w += Gm::NTHR)
+      U[(size_t)p * Gm::N + Gm::time_of_w(rank, w)] = cscale(s[Gm::sidx(Gm::local_of_w(w))], inv);
   }
 }
 
@@ -845,13 +857,13 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
     const int k = Gm::freq_of(rank, li);
     const double th = im_L(poly, d.n_beta, alpha_of(k, Gm::N, d.alpha_scale)) * z;
-    s[pad(li)] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
+    s[Gm::sidx(li)] = cmul(from_d2<T>(d.psi_hat[row + k]), expi<T>(th));
   }
   inverse<T, LOGN, XC>(s, sq, kp.tw);
 #pragma unroll 8
-  for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
-    const double2 r = to_d2(s[pad(u)]);
-    d.io[row + Gm::time_of(rank, u)] = make_double2(r.x * d.result_scale, r.y * d.result_scale);
+  for (int w = tid; w < Gm::NL; w += Gm::NTHR) {
+    const double2 r = to_d2(s[Gm::sidx(Gm::local_of_w(w))]);
+    d.io[row + Gm::time_of_w(rank, w)] = make_double2(r.x * d.result_scale, r.y * d.result_scale);
   }
 }
 
@@ -879,21 +891,21 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   const size_t row = (size_t)r * Gm::N;
   if constexpr (!INV) {
 #pragma unroll 8
-    for (int u = tid; u < Gm::NL; u += Gm::NTHR) s[pad(u)] = from_d2<T>(a.in[row + Gm::time_of(rank, u)]);
+    for (int w = tid; w < Gm::NL; w += Gm::NTHR) s[Gm::sidx(Gm::local_of_w(w))] = from_d2<T>(a.in[row + Gm::time_of_w(rank, w)]);
     forward<T, LOGN, XC>(s, sq, a.tw);
 #pragma unroll 8
     for (int li = tid; li < Gm::NL; li += Gm::NTHR) {
-      const double2 x = to_d2(s[pad(li)]);
+      const double2 x = to_d2(s[Gm::sidx(li)]);
       a.out[row + Gm::freq_of(rank, li)] = make_double2(x.x * a.scale, x.y * a.scale);
     }
   } else {
 #pragma unroll 8
-    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[pad(li)] = from_d2<T>(a.in[row + Gm::freq_of(rank, li)]);
+    for (int li = tid; li < Gm::NL; li += Gm::NTHR) s[Gm::sidx(li)] = from_d2<T>(a.in[row + Gm::freq_of(rank, li)]);
     inverse<T, LOGN, XC>(s, sq, a.tw);
 #pragma unroll 8
-    for (int u = tid; u < Gm::NL; u += Gm::NTHR) {
-      const double2 x = to_d2(s[pad(u)]);
-      a.out[row + Gm::time_of(rank, u)] = make_double2(x.x * a.scale, x.y * a.scale);
+    for (int w = tid; w < Gm::NL; w += Gm::NTHR) {
+      const double2 x = to_d2(s[Gm::sidx(Gm::local_of_w(w))]);
+      a.out[row + Gm::time_of_w(rank, w)] = make_double2(x.x * a.scale, x.y * a.scale);
     }
   }
 }
