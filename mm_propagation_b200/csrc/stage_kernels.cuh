@@ -546,8 +546,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   // psi_{n+1} = psi_n + h sum_j b_j N_j, src/MultimodePropagation_CPU.cpp:75-85) with
   // their coefficients h*a or h*b; N_hat_i itself comes from registers (cself).
   // Once the sigma loads are issued, the CTA's threads start L2 prefetches of the psi_hat
-  // and N_hat_j the cluster reads after its forward transform, so they arrive while the
-  // transform runs.
+  // the cluster reads after its forward transform, so it arrives while the transform runs.
   __shared__ int s_jq[kMaxStages];
   __shared__ double s_cq[kMaxStages];
   __shared__ int s_nq;
@@ -574,25 +573,16 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     }
     s_nq = nq;
   }
-  __syncthreads();  // s_jq, s_nq
   {
-    // the row's psi_hat and N_hat_j, 1/C of each per CTA of the cluster (together the
-    // frequencies every CTA reads), one 32 KB piece per thread
-    constexpr unsigned kNBytes = Gm::NL * (unsigned)sizeof(V);
-    constexpr unsigned kPiece = kNBytes < 32u * 1024u ? kNBytes : 32u * 1024u;
-    constexpr unsigned kPsiPieces = (Gm::NL * (unsigned)sizeof(double2)) / kPiece;
-    constexpr unsigned kNPieces = kNBytes / kPiece;
+    // the row's psi_hat, 1/C of it per CTA of the cluster (together the frequencies every
+    // CTA reads), one piece of at most 32 KB per thread. The N_hat_j are not prefetched:
+    // a wave's rows of them do not fit in L2 beside the rest, and measured, prefetching
+    // them too was slower.
+    constexpr unsigned kBytes = Gm::NL * (unsigned)sizeof(double2);
+    constexpr unsigned kPiece = kBytes < 32u * 1024u ? kBytes : 32u * 1024u;
     const size_t f0 = (size_t)p * Gm::N + (size_t)rank * Gm::NL;
-    const unsigned np = kPsiPieces + (unsigned)s_nq * kNPieces;
-    for (unsigned t = tid; t < np; t += Gm::NTHR) {
-      if (t < kPsiPieces) {
-        prefetch_l2(d.psi_hat + f0 + (size_t)t * (kPiece / sizeof(double2)), kPiece);
-      } else {
-        const unsigned u = t - kPsiPieces, q = u / kNPieces, pc = u - q * kNPieces;
-        prefetch_l2(as_t2<T>(d.Nh) + (size_t)s_jq[q] * ((size_t)d.M * Gm::N) + f0 + (size_t)pc * (kPiece / sizeof(V)),
-                    kPiece);
-      }
-    }
+    for (unsigned t = tid; t < kBytes / kPiece; t += Gm::NTHR)
+      prefetch_l2(d.psi_hat + f0 + (size_t)t * (kPiece / sizeof(double2)), kPiece);
   }
   cp_async_wait<0>();                  // this thread's sigma and twiddle copies
   forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers publish them and the values thread 0 wrote
