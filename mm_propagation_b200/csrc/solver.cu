@@ -1481,7 +1481,7 @@ bool batch_shape(mmp_batch* b) {
     const size_t sp = 2 * t2;  // one sample pair of one row
     const size_t rs = kSrSub / 2 + 1;
     const size_t plan = (size_t)((Mmax + kSrGroups - 1) / kSrGroups) * kSrGroups * sizeof(int4);
-    const size_t need = (2 * (size_t)Mmax + (size_t)Pall) * rs * sp + plan + max_sr_terms * (t2 + sizeof(unsigned));
+    const size_t need = (2 * (size_t)Mmax + (size_t)Pall) * rs * sp + plan + max_sr_terms * 2 * t2;  // SrRec
     if (ok && need <= 227 * 1024) {
       sr = true;
       pchunk = 0;

@@ -1609,6 +1609,26 @@ template <typename T> __device__ __forceinline__ void st_pair(SrPair<T>* p, c2<T
 }
 constexpr int kSrGroups = (kSrThreads / 32) * 4;  // groups of eight lanes in phase B
 
+// One merged term as k_contract_sr keeps it in shared memory: the coefficients (a, b) and
+// q | k << 16 in one record of 2 complex values (16 bytes in FP32, 32 in FP64), so that a
+// term costs one shared-memory access (two in FP64).
+template <typename T> struct SrRec {
+  c2<T> ab;
+  unsigned kq;
+  unsigned pad[sizeof(T) == 4 ? 1 : 3];
+};
+static_assert(sizeof(SrRec<float>) == 16 && sizeof(SrRec<double>) == 32, "SrRec layout");
+template <typename T> __device__ __forceinline__ void ld_rec(const SrRec<T>* r, c2<T>& ab, unsigned& kq) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(r);
+    ab = make_float2(v.x, v.y);
+    kq = __float_as_uint(v.z);
+  } else {
+    ab = r->ab;
+    kq = r->kq;
+  }
+}
+
 template <typename V> __device__ __forceinline__ V shfl_down_c(V v, int d) {
   v.x = __shfl_down_sync(0xffffffffu, v.x, d);
   v.y = __shfl_down_sync(0xffffffffu, v.y, d);
@@ -1632,18 +1652,19 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
   if (__ldcg(d.step) >= d.step_limit) return;     // finished solve (nothing is in flight yet)
   const int M = d.M, P = d.P, nterm = d.sr_terms, rounds = d.sr_rounds;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // shared memory: U [2][M][RS], W [P][RS], group plan [rounds kSrGroups], coefficients
-  // [nterm], q | k << 16 [nterm]
+  // shared memory: U [2][M][RS], W [P][RS], group plan [rounds kSrGroups], merged terms
+  // [nterm] (coefficients and q | k << 16)
   SP* sU = reinterpret_cast<SP*>(smem_raw);
   SP* sW = sU + 2 * (size_t)M * RS;
   int4* sPlan = reinterpret_cast<int4*>(sW + (size_t)P * RS);
-  CF* sCf = reinterpret_cast<CF*>(sPlan + rounds * kSrGroups);
-  unsigned* sKq = reinterpret_cast<unsigned*>(sCf + nterm);
+  SrRec<T>* sRec = reinterpret_cast<SrRec<T>*>(sPlan + rounds * kSrGroups);
   {
     const CF* gCf = static_cast<const CF*>(d.sr_coef);
     for (int i = tid; i < nterm; i += kSrThreads) {
-      sCf[i] = gCf[i];
-      sKq[i] = d.sr_kq[i];
+      SrRec<T> r = {};
+      r.ab = gCf[i];
+      r.kq = d.sr_kq[i];
+      sRec[i] = r;
     }
     for (int i = tid; i < rounds * kSrGroups; i += kSrThreads) sPlan[i] = d.sr_plan[i];
   }
@@ -1753,11 +1774,19 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
         // sigma = U X summed over the terms: Re = a1 - a2, Im = a3 + a4 with a1 = sum Re U Re X,
         // a2 = sum Im U Im X, a3 = sum Re U Im X, a4 = sum Im U Re X (packed over the pair)
         V a1 = mk<T>(0, 0), a2 = a1, a3 = a1, a4 = a1;
+        // a mode's terms are sorted by k: U_k is read again only when k changes
+        SP u = {};
+        int kprev = -1;
 #pragma unroll 2
         for (int n = pl.y; n < pl.z; ++n) {
-          const unsigned kq = sKq[n];
-          const CF c = sCf[n];
-          const SP u = ld_pair<T>(uc + (kq >> 16) * RS + j);
+          CF c;
+          unsigned kq;
+          ld_rec<T>(sRec + n, c, kq);
+          const int k = (int)(kq >> 16);
+          if (k != kprev) {
+            u = ld_pair<T>(uc + k * RS + j);
+            kprev = k;
+          }
           const SP w = ld_pair<T>(sW + (kq & 0xffffu) * RS + j);
           const V xr = pk_mul(mk<T>(c.x, c.x), w.re), xi = pk_mul(mk<T>(c.y, c.y), w.im);  // X
           a1 = pk_fma(u.re, xr, a1);
