@@ -186,13 +186,13 @@ template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   static constexpr int NTHR = NL / E;
   static constexpr int LOGCH = LOGNLG - LOGC;
   static constexpr int CH = 1 << LOGCH;  // frequencies per span: C G spans per CTA
-  static constexpr int LOGQ = LOGNLG - 2;  // quarter-wave twiddle table of the local size
+  static constexpr int LOGH = LOGNLG - 1;  // half-wave twiddle table of the local size
   // rows g > 0 start SKEW elements later (mod 128 bytes), so that a warp walking the
   // samples in time order (row g = lane mod G) reads and writes without bank conflicts
   static constexpr int SKEW = LOGG > 0 ? 4 : 0;
   static constexpr int DATA_BYTES = (padded_len(NL) + (G - 1) * SKEW) * (int)sizeof(c2<T>);
-  static constexpr int TWQ_BYTES = padded_len(NLG / 4) * (int)sizeof(c2<T>);
-  static constexpr int SMEM_BYTES = DATA_BYTES + TWQ_BYTES;
+  static constexpr int TW_BYTES = padded_len(NLG / 2) * (int)sizeof(c2<T>);
+  static constexpr int SMEM_BYTES = DATA_BYTES + TW_BYTES;
   // split rows (XC_ > 0) are sized so that two CTAs share an SM
   static constexpr int MIN_BLOCKS = (XC_ > 0 && SMEM_BYTES <= 110 * 1024 && NTHR <= 512) ? 2 : 1;
   static_assert(LOGE >= LOGC + LOGG, "each thread must combine at least one frequency per CTA");
@@ -220,35 +220,34 @@ template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   }
 };
 
-// exp(-2 pi i m / NL) (conjugated for INV) from the quarter-wave table
-// sq[pad(m')] = exp(-2 pi i m' / NL), m' < NL/4: w(m) = (-i)^(m div NL/4) * sq[m mod NL/4].
+// exp(-2 pi i m / NLG) (conjugated for INV) from the half-wave table
+// sh[pad(m')] = exp(-2 pi i m' / NLG), m' < NLG/2: w(m) = -sh[m - NLG/2] from NLG/2 on.
 // The table uses the same padded index as the data: the Stockham passes read it at
 // strides of 2^a entries, which would otherwise land in one bank.
-template <typename V, bool INV, int LOGQ>
-__device__ __forceinline__ V tw_quarter(const V* __restrict__ sq, int m) {
-  const int q = m >> LOGQ;
-  const V w = sq[pad(m & ((1 << LOGQ) - 1))];
-  V r;
-  r.x = (q & 1) ? w.y : w.x;
-  r.y = (q & 1) ? -w.x : w.y;
-  if (q & 2) { r.x = -r.x; r.y = -r.y; }
-  if (INV) r.y = -r.y;
-  return r;
+template <typename V, bool INV, int LOGH>
+__device__ __forceinline__ V tw_half(const V* __restrict__ sh, int m) {
+  V w = sh[pad(m & ((1 << LOGH) - 1))];
+  if (m >> LOGH) { w.x = -w.x; w.y = -w.y; }
+  if (INV) w.y = -w.y;
+  return w;
 }
 
-// Copy the first quarter of the local transform's table (NLG points) into shared memory.
+// Copy the first half of the local transform's table (NLG points) into shared memory.
 template <typename T, int LOGN, int XC>
 __device__ __forceinline__ c2<T>* load_twiddles(unsigned char* smem_raw, const TwTables& tw) {
   using Gm = Geo<T, LOGN, XC>;
   c2<T>* sq = reinterpret_cast<c2<T>*>(smem_raw + Gm::DATA_BYTES);
   const c2<T>* g = tw_table<T>(tw, Gm::LOGNLG);
 #pragma unroll 4
-  for (int m = threadIdx.x; m < Gm::NLG / 4; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
+  for (int m = threadIdx.x; m < Gm::NLG / 2; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
   return sq;
 }
 
 // One in-place Stockham pass of radix 2^LOGR at stride Ns = 2^logns (runtime) over the
 // rows of Gm (G rows of NLG samples; a thread's butterflies j < NL/R, row j / (NLG/R)).
+// Shared-memory offsets: where a butterfly's R elements lie 32·c apart within a row, the
+// padded offset advances by a constant (pad(i + 32c) = pad(i) + 33c), so only the first
+// is computed.
 template <typename Gm, int LOGR, bool INV>
 __device__ __forceinline__ void stockham_pass(c2<typename Gm::Real>* __restrict__ s,
                                               const c2<typename Gm::Real>* __restrict__ sq, int logns) {
@@ -257,14 +256,21 @@ __device__ __forceinline__ void stockham_pass(c2<typename Gm::Real>* __restrict_
   constexpr int NB = 1 << LOGB, E = Gm::E, NTHR = Gm::NTHR;
   constexpr int R = 1 << LOGR, NBF = E / R;
   constexpr int LOGJ = LOGB - LOGR;  // butterflies per row
+  constexpr int S = NB / R;          // read stride
   const int tid = threadIdx.x;
   V v[E];
 #pragma unroll
   for (int bf = 0; bf < NBF; ++bf) {
     const int ja = tid + bf * NTHR;
     const int base = (ja >> LOGJ) << LOGB, j = ja & ((1 << LOGJ) - 1);
+    if constexpr (S % 32 == 0) {
+      const int a0 = Gm::sidx(base + j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[bf * R + r] = s[Gm::sidx(base + j + r * (NB / R))];
+      for (int r = 0; r < R; ++r) v[bf * R + r] = s[a0 + r * (S + S / 32)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[bf * R + r] = s[Gm::sidx(base + j + r * S)];
+    }
   }
   __syncthreads();
   const int nsm = (1 << logns) - 1;
@@ -276,12 +282,22 @@ __device__ __forceinline__ void stockham_pass(c2<typename Gm::Real>* __restrict_
     if (logns > 0) {
       const int step = jm << (LOGB - logns - LOGR);  // jm * NB / (Ns * R)
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_quarter<V, INV, Gm::LOGQ>(sq, r * step));
+      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_half<V, INV, Gm::LOGH>(sq, r * step));
     }
     RegDFT<R, INV>::run(&v[bf * R]);
     const int idxD = ((j >> logns) << (logns + LOGR)) + jm;
+    const int w0 = Gm::sidx(base + idxD);
+    if (logns >= 5) {  // R elements Ns apart, Ns a multiple of 32
+      const int st = (1 << logns) + (1 << (logns - 5));
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[Gm::sidx(base + idxD + (r << logns))] = v[bf * R + r];
+      for (int r = 0; r < R; ++r) s[w0 + r * st] = v[bf * R + r];
+    } else if (logns == 0) {  // R consecutive elements from a multiple of R (R <= 32)
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[w0 + r] = v[bf * R + r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[Gm::sidx(base + idxD + (r << logns))] = v[bf * R + r];
+    }
   }
   __syncthreads();
 }

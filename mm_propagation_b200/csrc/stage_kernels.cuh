@@ -180,7 +180,7 @@ template <typename G> __device__ __forceinline__ int cluster_rank() {
   else return (int)cg::this_cluster().block_rank();
 }
 
-// Common start of a row kernel: shared memory, the quarter-wave twiddle table.
+// Common start of a row kernel: shared memory (the row, then the half-wave twiddle table).
 #define MMP_ROW_SMEM()                                                 \
   extern __shared__ __align__(16) unsigned char smem_raw[];            \
   V* s = reinterpret_cast<V*>(smem_raw);
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   V* sq = reinterpret_cast<V*>(smem_raw + Gm::DATA_BYTES);
   {
     const c2<T>* g = tw_table<T>(kp.tw, Gm::LOGNLG);
-    for (int m = tid; m < Gm::NLG / 4; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
+    for (int m = tid; m < Gm::NLG / 2; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
     const SolveDesc* gd = kp.descs + blockIdx.y;
     if (p < __ldg(&gd->M)) {
       const V* sg = as_t2<T>(reinterpret_cast<const void*>(__ldg(reinterpret_cast<const unsigned long long*>(&gd->sigma)))) +

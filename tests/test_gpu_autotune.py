@@ -61,6 +61,26 @@ def test_every_row_split_candidate_matches_oracle(mmp, monkeypatch, nt):
     assert ctas[1] == 2 * ctas[0]
 
 
+@pytest.mark.parametrize("fp64,nt", [(False, 4096), (False, 8192), (False, 32768), (True, 2048), (True, 4096),
+                                     (True, 8192), (True, 16384)])
+def test_every_split_row_geometry_matches_oracle(mmp, monkeypatch, fp64, nt):
+    # the row-split variants not covered above: rows dealt out to 2, 4 or 8 CTAs in runs
+    # of 32 bytes (4 FP32 or 2 FP64 samples), combined by one radix-(C G) butterfly
+    from mm_propagation_b200 import capi
+    prob = W.small_case(seed=151, M=2, nt=nt, n_steps=3, window=40.0 if nt >= 16384 else 10.0, nnz_target=8)
+    ref = mo.solve(prob)
+    prob = prob.replace(flags=prob.flags | (capi.MMP_F_FP64 if fp64 else 0))
+    ctas = []
+    for xc in (0, 1):
+        monkeypatch.setenv("MMP_ROW_SPLIT", str(xc))
+        with mmp.Solver(prob) as s:
+            s.propagate(prob.n_steps)
+            out, info = s.result(), s.info()
+        ctas.append(info["cluster_ctas"])
+        assert mo.rel_l2_per_mode(out, ref).max() < (1e-11 if fp64 else TOL32), xc
+    assert ctas[1] == 2 * ctas[0]
+
+
 def test_tuned_choice_is_reported_cached_and_leaves_no_trace(mmp, monkeypatch):
     probs = [_tall(160 + i) for i in range(4)]
     outs, info = _batch_run(mmp, probs, 3)  # tuned here (or taken from the cache)
