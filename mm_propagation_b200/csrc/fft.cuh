@@ -186,12 +186,17 @@ template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   static constexpr int NTHR = NL / E;
   static constexpr int LOGCH = LOGNLG - LOGC;
   static constexpr int CH = 1 << LOGCH;  // frequencies per span: C G spans per CTA
-  static constexpr int LOGH = LOGNLG - 1;  // half-wave twiddle table of the local size
+  // twiddle table of the local size in shared memory: half a wave (one sign flip per
+  // lookup) where that is at most 32 KB, else a quarter wave (a quadrant fold per lookup;
+  // a 64 KB table cost the 16384-sample single-CTA rows ~5% in loading it)
+  static constexpr bool TW_HALF = (NLG / 2) * (int)sizeof(c2<T>) <= 32 * 1024;
+  static constexpr int LOGH = TW_HALF ? LOGNLG - 1 : LOGNLG - 2;  // log2 of the table's entries
+  static constexpr int NTW = 1 << LOGH;
   // rows g > 0 start SKEW elements later (mod 128 bytes), so that a warp walking the
   // samples in time order (row g = lane mod G) reads and writes without bank conflicts
   static constexpr int SKEW = LOGG > 0 ? 4 : 0;
   static constexpr int DATA_BYTES = (padded_len(NL) + (G - 1) * SKEW) * (int)sizeof(c2<T>);
-  static constexpr int TW_BYTES = padded_len(NLG / 2) * (int)sizeof(c2<T>);
+  static constexpr int TW_BYTES = padded_len(NTW) * (int)sizeof(c2<T>);
   static constexpr int SMEM_BYTES = DATA_BYTES + TW_BYTES;
   // split rows (XC_ > 0) are sized so that two CTAs share an SM
   static constexpr int MIN_BLOCKS = (XC_ > 0 && SMEM_BYTES <= 110 * 1024 && NTHR <= 512) ? 2 : 1;
@@ -220,26 +225,35 @@ template <typename T, int LOGN_, int XC_ = 0> struct Geo {
   }
 };
 
-// exp(-2 pi i m / NLG) (conjugated for INV) from the half-wave table
-// sh[pad(m')] = exp(-2 pi i m' / NLG), m' < NLG/2: w(m) = -sh[m - NLG/2] from NLG/2 on.
+// exp(-2 pi i m / NLG) (conjugated for INV), m < NLG, from the table
+// sh[pad(m')] = exp(-2 pi i m' / NLG), m' < 2^LOGH: a half wave (w(m) = -sh[m - NLG/2] from
+// NLG/2 on) or a quarter wave (w(m) = (-i)^(m div NLG/4) sh[m mod NLG/4]).
 // The table uses the same padded index as the data: the Stockham passes read it at
 // strides of 2^a entries, which would otherwise land in one bank.
-template <typename V, bool INV, int LOGH>
-__device__ __forceinline__ V tw_half(const V* __restrict__ sh, int m) {
+template <typename V, bool INV, bool HALF, int LOGH>
+__device__ __forceinline__ V tw_lookup(const V* __restrict__ sh, int m) {
+  const int q = m >> LOGH;
   V w = sh[pad(m & ((1 << LOGH) - 1))];
-  if (m >> LOGH) { w.x = -w.x; w.y = -w.y; }
+  if constexpr (HALF) {
+    if (q) { w.x = -w.x; w.y = -w.y; }
+  } else {
+    const V w0 = w;
+    w.x = (q & 1) ? w0.y : w0.x;
+    w.y = (q & 1) ? -w0.x : w0.y;
+    if (q & 2) { w.x = -w.x; w.y = -w.y; }
+  }
   if (INV) w.y = -w.y;
   return w;
 }
 
-// Copy the first half of the local transform's table (NLG points) into shared memory.
+// Copy the first 2^LOGH entries of the local transform's table (NLG points) into shared memory.
 template <typename T, int LOGN, int XC>
 __device__ __forceinline__ c2<T>* load_twiddles(unsigned char* smem_raw, const TwTables& tw) {
   using Gm = Geo<T, LOGN, XC>;
   c2<T>* sq = reinterpret_cast<c2<T>*>(smem_raw + Gm::DATA_BYTES);
   const c2<T>* g = tw_table<T>(tw, Gm::LOGNLG);
 #pragma unroll 4
-  for (int m = threadIdx.x; m < Gm::NLG / 2; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
+  for (int m = threadIdx.x; m < Gm::NTW; m += Gm::NTHR) sq[pad(m)] = __ldg(&g[m]);
   return sq;
 }
 
@@ -282,7 +296,7 @@ __device__ __forceinline__ void stockham_pass(c2<typename Gm::Real>* __restrict_
     if (logns > 0) {
       const int step = jm << (LOGB - logns - LOGR);  // jm * NB / (Ns * R)
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_half<V, INV, Gm::LOGH>(sq, r * step));
+      for (int r = 1; r < R; ++r) v[bf * R + r] = cmul(v[bf * R + r], tw_lookup<V, INV, Gm::TW_HALF, Gm::LOGH>(sq, r * step));
     }
     RegDFT<R, INV>::run(&v[bf * R]);
     const int idxD = ((j >> logns) << (logns + LOGR)) + jm;

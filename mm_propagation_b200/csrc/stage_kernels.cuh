@@ -180,7 +180,7 @@ template <typename G> __device__ __forceinline__ int cluster_rank() {
   else return (int)cg::this_cluster().block_rank();
 }
 
-// Common start of a row kernel: shared memory (the row, then the half-wave twiddle table).
+// Common start of a row kernel: shared memory (the row, then the twiddle table).
 #define MMP_ROW_SMEM()                                                 \
   extern __shared__ __align__(16) unsigned char smem_raw[];            \
   V* s = reinterpret_cast<V*>(smem_raw);
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   V* sq = reinterpret_cast<V*>(smem_raw + Gm::DATA_BYTES);
   {
     const c2<T>* g = tw_table<T>(kp.tw, Gm::LOGNLG);
-    for (int m = tid; m < Gm::NLG / 2; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
+    for (int m = tid; m < Gm::NTW; m += Gm::NTHR) cp_async_c2<T>(&sq[pad(m)], &g[m]);
     const SolveDesc* gd = kp.descs + blockIdx.y;
     if (p < __ldg(&gd->M)) {
       const V* sg = as_t2<T>(reinterpret_cast<const void*>(__ldg(reinterpret_cast<const unsigned long long*>(&gd->sigma)))) +
@@ -615,8 +615,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   auto body = [&](auto nqc, int nqr) {
     constexpr int NQ = decltype(nqc)::value;
     // frequencies per chunk: all of a chunk's loads are in flight together (8 when the
-    // stage reads only psi_hat)
-    constexpr int CHK0 = NQ == 0 ? 8 : (NQ <= 3 ? 4 : 2);
+    // stage reads only psi_hat; 4 also with 4 or 5 stored terms, where 2 was measured 3%
+    // slower on the 28-mode sweep and 2% on the 6-mode order-6 batch)
+    constexpr int CHK0 = NQ == 0 ? 8 : 4;
     constexpr int CHK = CHK0 < Gm::E ? CHK0 : Gm::E;
     const double nb3 = d.n_beta == 3;
 #pragma unroll 1
