@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #ifndef MMP_NO_NVTX
@@ -581,18 +582,29 @@ void host_setup(const mmp_params* p, Member& s) {
     me = (int)(src / M);
     return std::make_pair(std::min(le, me), std::max(le, me));
   };
-  // the pair fields the non-zero terms read, numbered in (l, m) order: neighbouring pair
-  // fields then mostly share l and have distinct m, which keeps the one-pair-field-per-lane
-  // loads of k_contract_sr and k_raman_agg_sr free of shared-memory bank conflicts
+  // the pair fields the non-zero terms read, numbered block by block over the (l, m)
+  // triangle, blocks of 8 l by 2 m: a warp's 32 consecutive pair fields (one per lane in
+  // k_contract_sr and k_raman_agg_sr) then read few distinct U rows, whose 16-byte loads
+  // share wavefronts (the rows start 4 banks apart). Measured on the 28-mode sweep against
+  // (l, m) order: k_raman_agg_sr 0.544 -> 0.469 ms, k_contract_sr 2.08 -> 2.02 ms.
   std::map<std::pair<int, int>, int> pair_idx;
   for (uint32_t q = 0; q < M; ++q)
     for (const mmp_nz* e : byp[q]) {
       int le, me;
       if (e->value != 0.0) pair_idx[pair_of(e, le, me)] = 0;
     }
-  for (auto& kv : pair_idx) {
-    kv.second = (int)s.pairs.size();
-    s.pairs.push_back(make_int2(kv.first.first, kv.first.second));
+  {
+    std::vector<std::pair<int, int>> order;
+    for (const auto& kv : pair_idx) order.push_back(kv.first);
+    auto key = [](const std::pair<int, int>& x) {
+      return std::make_tuple(x.first / 8, x.second / 2, x.first % 8, x.second % 2);
+    };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](const std::pair<int, int>& a, const std::pair<int, int>& b) { return key(a) < key(b); });
+    for (const auto& lm : order) {
+      pair_idx[lm] = (int)s.pairs.size();
+      s.pairs.push_back(make_int2(lm.first, lm.second));
+    }
   }
   s.term_off.assign(M + 1, 0);
   for (uint32_t q = 0; q < M; ++q) {
