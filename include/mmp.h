@@ -162,7 +162,9 @@ int mmp_get_result(mmp_solver* s, double* out);
 
 /* Replace the field with new initial fields phi0[M][NT][2] (W^(1/2)) and set z = 0,
  * keeping every other parameter: the same as constructing a new solver with
- * other initial_fields, without re-uploading the rest. */
+ * other initial_fields, without re-uploading the rest. The fields are checked for
+ * NaN/Inf on the device copy before anything of the solve changes (MMP_EINVAL then);
+ * the call returns once they are on the device (it waits for the solver's stream). */
 int mmp_set_fields(mmp_solver* s, const double* phi0);
 
 /* Per-step FP64 monitors since creation: total energy (pJ, sum over modes of

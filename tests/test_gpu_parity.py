@@ -139,6 +139,24 @@ def test_energy_monitor_conserved_without_raman(mmp):
     assert np.abs(e / e[0] - 1).max() < 1e-6
 
 
+def test_set_fields_rejects_nonfinite_and_keeps_the_solve(mmp):
+    # set_fields checks the fields on the device copy, before any of the solve's state changes
+    prob = W.small_case(seed=90, M=3, nt=1024, n_steps=4)
+    ref = mo.solve(prob)
+    bad = prob.initial_fields.copy()
+    bad[1, 17] = np.inf
+    with mmp.Solver(prob) as s:
+        for v in (np.nan, np.inf):
+            bad[1, 17] = v
+            with pytest.raises(mmp.MMPError) as ei:
+                s.set_fields(bad)
+            assert ei.value.code == capi.MMP_EINVAL
+            assert "not finite" in mmp.lib().mmp_last_error().decode()
+        s.propagate(prob.n_steps)
+        out = s.result()
+    assert mo.rel_l2_per_mode(out, ref).max() < TOL32
+
+
 def test_nonfinite_is_reported(mmp):
     # the literal reading of the four-entry pattern diverges (see workloads.grin2)
     prob = W.grin2(seed=1, nt=256, n_steps=1000, literal=True)
