@@ -262,11 +262,14 @@ def stage_bytes(prob, tab_s, a, b, bt, pairs, raman_path):
     nu = 0.0
     for i in range(tab_s):
         last = i == tab_s - 1
-        rows = 3 * M * bt + M * 16                     # read sigma, write N_i, write U; read psi_hat
+        rows = 3 * M * bt                              # read sigma, write N_i, write U
         if last:
-            rows += M * 16 + sum(1 for j in range(tab_s) if b[j] != 0 and j != i) * M * bt
+            # read and write psi_hat (FP64), write its copy in T (FP32 solves), read the N_j
+            rows += 2 * M * 16 + (M * bt if bt == 8 else 0)
+            rows += sum(1 for j in range(tab_s) if b[j] != 0 and j != i) * M * bt
         else:
-            rows += sum(1 for j in range(i) if a[i + 1][j] != 0) * M * bt  # N_i is in registers
+            # read psi_hat's copy in T (psi_hat itself in FP64), read the stored N_j
+            rows += M * bt + sum(1 for j in range(i) if a[i + 1][j] != 0) * M * bt  # N_i is in registers
         nu += rows * NT
     return {"pair": pair, "contract": contract, "nu": nu / tab_s}
 

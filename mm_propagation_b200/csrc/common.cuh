@@ -93,6 +93,9 @@ struct SolveDesc {
   double photon_scale;
   const double* poly;   // [M][n_beta]: Im L_p(alpha) = sum_j poly[p][j] alpha^j
   double2* psi_hat;     // [M][NT] interaction-picture field, frequency domain, FP64
+  // [M][NT] psi_hat rounded to T, written wherever psi_hat is (the intermediate stages
+  // read it: they round psi_hat to T anyway); psi_hat itself in FP64 solves
+  void* psi_t;
   void* Nh;             // [s][M][NT] stage derivatives, frequency domain (T2)
   void* U;              // [M][NT] stage field, time domain (T2)
   void* W;              // [P][NT] Raman-convolved pair fields R, time domain (T2)

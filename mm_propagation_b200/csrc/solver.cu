@@ -1060,6 +1060,13 @@ int member_set_fields(mmp_batch* b, uint32_t idx, const double* phi0) {
   void* args[] = {&a};
   CUDA_TRY(launch(b->ks64.dft_fwd, dim3((unsigned)(s.M * b->ks64.C), 1, 1), b->ks64.nthr, b->ks64.smem,
                   b->ks64.C, b->stream, args));
+  if (!b->fp64) {  // psi_hat rounded to T
+    const double2* src = s.desc.psi_hat;
+    float2* dst = (float2*)s.desc.psi_t;
+    size_t n = (size_t)s.M * s.nt;
+    void* cargs[] = {(void*)&src, &dst, &n};
+    CUDA_TRY(launch((const void*)&k_to_t2<float>, dim3(1184, 1, 1), 256, 0, 1, b->stream, cargs));
+  }
   CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), b->stream));  // z = 0
   CUDA_TRY(cudaMemsetAsync((char*)s.counters + 3 * sizeof(unsigned long long), 0, sizeof(int), b->stream));
   // the drift check's reference energy: the first step's energy from these fields on
@@ -1165,6 +1172,7 @@ size_t member_bytes(const mmp_batch* b, const Member& s) {
   const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
   size_t off = 0;
   off = align_up(off + M * nt * sizeof(double2));                               // psi_hat
+  off = align_up(off + (b->fp64 ? 0 : M * nt * t2));                            // psi_hat in T
   off = align_up(off + M * nt * sizeof(double2));                               // io
   off = align_up(off + S * M * nt * t2);                                        // Nh
   off = align_up(off + M * nt * t2);                                            // U
@@ -1227,9 +1235,11 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   host_setup(p, s);
   const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
   const size_t nt = b->nt, M = s.M, P = s.pairs.size(), S = (size_t)b->tab.s;
-  // one allocation: psi_hat | io | Nh | U | sigma | W | H | tiles | poly | pairs | terms | term_off | counters
+  // one allocation: psi_hat | psi_hat in T | io | Nh | U | sigma | W | H | tiles | poly | pairs | terms |
+  // term_off | counters
   size_t off = 0;
   const size_t o_psi = off; off = align_up(off + M * nt * sizeof(double2));
+  const size_t o_pst = off; off = align_up(off + (b->fp64 ? 0 : M * nt * t2));
   const size_t o_io = off; off = align_up(off + M * nt * sizeof(double2));
   const size_t o_nh = off; off = align_up(off + S * M * nt * t2);
   const size_t o_u = off; off = align_up(off + M * nt * t2);
@@ -1275,6 +1285,7 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
   d.photon_scale = d.energy_scale * s.T0 / 1.054571817e-10;
   d.poly = (const double*)T2ptr(s.block, o_poly);
   d.psi_hat = (double2*)T2ptr(s.block, o_psi);
+  d.psi_t = b->fp64 ? (void*)d.psi_hat : T2ptr(s.block, o_pst);
   d.io = (double2*)T2ptr(s.block, o_io);
   d.Nh = T2ptr(s.block, o_nh);
   d.U = T2ptr(s.block, o_u);

@@ -574,15 +574,17 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     s_nq = nq;
   }
   {
-    // the row's psi_hat, 1/C of it per CTA of the cluster (together the frequencies every
-    // CTA reads), one piece of at most 32 KB per thread. The N_hat_j are not prefetched:
-    // a wave's rows of them do not fit in L2 beside the rest, and measured, prefetching
-    // them too was slower.
-    constexpr unsigned kBytes = Gm::NL * (unsigned)sizeof(double2);
-    constexpr unsigned kPiece = kBytes < 32u * 1024u ? kBytes : 32u * 1024u;
-    const size_t f0 = (size_t)p * Gm::N + (size_t)rank * Gm::NL;
-    for (unsigned t = tid; t < kBytes / kPiece; t += Gm::NTHR)
-      prefetch_l2(d.psi_hat + f0 + (size_t)t * (kPiece / sizeof(double2)), kPiece);
+    // the row's psi_hat (FP64 at the last stage, in T at the others), 1/C of it per CTA of
+    // the cluster (together the frequencies every CTA reads), one piece of at most 32 KB
+    // per thread. The N_hat_j are not prefetched: a wave's rows of them do not fit in L2
+    // beside the rest, and measured, prefetching them too was slower.
+    const bool lastp = kp.stage == kp.tab.s - 1;
+    const unsigned esz = lastp ? (unsigned)sizeof(double2) : (unsigned)sizeof(V);
+    const unsigned bytes = Gm::NL * esz;
+    const unsigned piece = bytes < 32u * 1024u ? bytes : 32u * 1024u;
+    const char* base = reinterpret_cast<const char*>(lastp ? (const void*)d.psi_hat : d.psi_t) +
+                       ((size_t)p * Gm::N + (size_t)rank * Gm::NL) * esz;
+    for (unsigned t = tid; t < bytes / piece; t += Gm::NTHR) prefetch_l2(base + (size_t)t * piece, piece);
   }
   cp_async_wait<0>();                  // this thread's sigma and twiddle copies
   forward<T, LOGN, XC>(s, sq, kp.tw);  // its barriers publish them and the values thread 0 wrote
@@ -595,6 +597,10 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   const size_t row = (size_t)p * Gm::N;
   const size_t mstride = (size_t)d.M * Gm::N;
   V* Nh = as_t2<T>(d.Nh);
+  V* psiT = as_t2<T>(d.psi_t);
+  // FP32 stage bodies of one kind read psi_hat's T copy at the intermediate stages; the
+  // FP64 ones (psi_t is psi_hat) and the any-stage body read psi_hat
+  constexpr bool kReadT = sizeof(T) == 4 && BODY >= 0;
   const double zi = s_z[0], znext = s_z[1];
   double e_part = 0.0, p_part = 0.0;
   bool finite = true;
@@ -623,14 +629,17 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
 #pragma unroll 1
     for (int e0 = 0; e0 < Gm::E; e0 += CHK) {
       int kk[CHK];
-      double2 ps[CHK];
+      double2 ps[CHK];  // last stage: psi_hat in FP64
+      V pt[CHK];        // other stages: psi_hat in T
       V sv[CHK];
       V nj[CHK][NQ > 0 ? NQ : 1];
 #pragma unroll
       for (int c = 0; c < CHK; ++c) {
         const int li = tid + (e0 + c) * Gm::NTHR;
         kk[c] = Gm::freq_of(rank, li);
-        ps[c] = d.psi_hat[row + kk[c]];
+        if constexpr (!kReadT) ps[c] = d.psi_hat[row + kk[c]];
+        else if (last) ps[c] = d.psi_hat[row + kk[c]];
+        else pt[c] = psiT[row + kk[c]];
         sv[c] = s[Gm::sidx(li)];
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
@@ -669,6 +678,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
           finite = finite && isfinite(a2);
           e_part += a2;
           xt = from_d2<T>(x);
+          psiT[row + k] = xt;
           // photon monitor in FP32 (per-thread partial sums; FP64 across threads)
           if (w0f != 0.0f) {
             const int kk = (k <= (Gm::N >> 1)) ? k : k - Gm::N;
@@ -695,7 +705,8 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
           if (d.omega0_T0 != 0.0) p_part += a2 / (d.omega0_T0 + alpha);
           xt = from_d2<T>(x);
         } else {
-          xt = from_d2<T>(ps[c]);
+          if constexpr (!kReadT) xt = from_d2<T>(ps[c]);
+          else xt = pt[c];  // = psi_hat rounded to T
           const T cs = (T)cself;
           xt.x = fma(cs, nh.x, xt.x);
           xt.y = fma(cs, nh.y, xt.y);
@@ -751,6 +762,7 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
         }
       }
       d.psi_hat[row + k] = x;
+      if constexpr (sizeof(T) == 4) psiT[row + k] = from_d2<T>(x);
       const double a2 = x.x * x.x + x.y * x.y;
       finite = finite && isfinite(a2);
       e_part += a2;
