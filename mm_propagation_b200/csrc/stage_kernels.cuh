@@ -533,8 +533,15 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
   stage_desc(&sdesc, kp.descs + blockIdx.y);
   __syncthreads();
   const SolveDesc& d = sdesc;
-  if (p >= d.M || __ldcg(d.step) >= d.step_limit) {  // uniform over the cluster
+  if (p >= d.M) {  // empty slot (its descriptor is zero); uniform over the cluster
     cp_async_wait<0>();  // no copy may land after the CTA has left
+    return;
+  }
+  // the step counters in one round trip, shared by the finished-solve check and thread
+  // 0's setup below
+  const unsigned long long n_step = __ldcg(d.step), n_total = __ldcg(d.total);
+  if (n_step >= d.step_limit) {  // finished solve; uniform over the cluster
+    cp_async_wait<0>();
     return;
   }
   load_poly(poly, d, p);
@@ -555,12 +562,9 @@ __global__ void __launch_bounds__(Geo<T, LOGN, XC>::NTHR, Geo<T, LOGN, XC>::MIN_
     const int S = kp.tab.s;
     const bool last = (i == S - 1);
     const double h = d.dz;
-    const size_t row = (size_t)p * Gm::N;
-    const size_t mstride = (size_t)d.M * Gm::N;
-    const V* Nh = as_t2<T>(d.Nh);
-    const unsigned long long n = __ldcg(d.step);
+    const unsigned long long n = n_step;
     s_cnt[0] = n;
-    s_cnt[1] = __ldcg(d.total);
+    s_cnt[1] = n_total;
     s_z[0] = ((double)n + kp.tab.c[i]) * h;
     s_z[1] = last ? ((double)(n + 1)) * h : ((double)n + kp.tab.c[i + 1]) * h;
     int nq = 0;
