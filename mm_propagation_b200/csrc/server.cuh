@@ -234,7 +234,10 @@ bool admit_waiting(mmp_server* sv) {
     if (rc == MMP_OK) {
       for (size_t i = 0; i < sv->pools.size(); ++i) {
         Pool& pl = sv->pools[i];
-        if (pl.used >= (int)pl.b->capacity || !same_shape(pl.b, &r->p)) continue;
+        // a request joins only a pool where it runs the kernels and tiles it runs alone,
+        // so its fields are those of a standalone solve whatever it shares the pool with
+        if (pl.used >= (int)pl.b->capacity || !same_shape(pl.b, &r->p) || !joins_same_kernels(pl.b, &r->p))
+          continue;
         if (pl.in_flight) {
           deferred = true;  // a pool with room is busy: try again after its replay
           continue;

@@ -1423,28 +1423,59 @@ int member_init(mmp_batch* b, uint32_t idx, const mmp_params* p) {
 
 // Launch geometry that depends on the members: largest M and P, contraction tile and
 // its shared memory. Returns true when it changed (captured graphs are then stale).
-bool batch_shape(mmp_batch* b) {
-  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
-  int Mmax = 0, Pmax = 0, Pall = 0;
-  uint32_t span = 0;
+// What a batch's launch shape depends on: maxima (and minima) over its solves.
+struct ShapeStats {
+  int Mmax = 0, Mmin = 1 << 30, Pmax = 0, Pall = 0;
   size_t max_terms = 0, max_sr_terms = 0;
-  bool iir = b->raman;
-  bool all_dense = true, any_dense = false;
-  int Mmin = 1 << 30;
-  for (size_t i = 0; i < b->members.size(); ++i) {
-    if (!b->active[i]) continue;
-    const Member& s = b->members[i];
-    iir = iir && s.desc.iir;
-    all_dense = all_dense && s.dense_ok;
-    any_dense = any_dense || s.dense_ok;
-    span = (uint32_t)i + 1;
-    Mmax = std::max(Mmax, (int)s.M);
-    Mmin = std::min(Mmin, (int)s.M);
-    Pmax = std::max(Pmax, (int)(b->raman ? s.pairs.size() : 0));
-    Pall = std::max(Pall, (int)s.pairs.size());
-    max_terms = std::max(max_terms, s.terms.size());
-    max_sr_terms = std::max(max_sr_terms, s.sr_kq.size());
-  }
+  bool iir = true, all_dense = true, any_dense = false;
+  uint32_t span = 0;
+};
+
+void add_stats(ShapeStats& st, const mmp_batch* b, const Member& s, bool iir, bool dense_ok, uint32_t span) {
+  st.iir = st.iir && iir;
+  st.all_dense = st.all_dense && dense_ok;
+  st.any_dense = st.any_dense || dense_ok;
+  st.span = std::max(st.span, span);
+  st.Mmax = std::max(st.Mmax, (int)s.M);
+  st.Mmin = std::min(st.Mmin, (int)s.M);
+  st.Pmax = std::max(st.Pmax, (int)(b->raman ? s.pairs.size() : 0));
+  st.Pall = std::max(st.Pall, (int)s.pairs.size());
+  st.max_terms = std::max(st.max_terms, s.terms.size());
+  st.max_sr_terms = std::max(st.max_sr_terms, s.sr_kq.size());
+}
+
+ShapeStats batch_stats(const mmp_batch* b) {
+  ShapeStats st;
+  for (size_t i = 0; i < b->members.size(); ++i)
+    if (b->active[i]) {
+      const Member& s = b->members[i];
+      add_stats(st, b, s, s.desc.iir != 0, s.dense_ok, (uint32_t)i + 1);
+    }
+  return st;
+}
+
+// A batch's launch shape: the contraction form and tile, the Raman route and the shared
+// memory they take, chosen from its statistics alone.
+struct Shape {
+  int Mmax = 0, Pmax = 0, TT = 32, dense = 0, pchunk = 0, stage_terms = 0;
+  bool tc = false, sr = false, fused = false, iir = false;
+  size_t smem = 0;
+  uint32_t span = 0;
+};
+
+// Shapes that run the same kernels with the same tiles on a solve (so give it the same bits).
+bool same_kernels(const Shape& x, const Shape& y) {
+  return x.TT == y.TT && x.dense == y.dense && x.pchunk == y.pchunk && x.stage_terms == y.stage_terms &&
+         x.tc == y.tc && x.sr == y.sr && x.fused == y.fused && x.iir == y.iir;
+}
+
+Shape choose_shape(const mmp_batch* b, const ShapeStats& st) {
+  const size_t t2 = b->fp64 ? sizeof(double2) : sizeof(float2);
+  const int Mmax = st.Mmax, Pmax = st.Pmax, Pall = st.Pall, Mmin = st.Mmin;
+  const uint32_t span = st.span;
+  const size_t max_terms = st.max_terms, max_sr_terms = st.max_sr_terms;
+  bool iir = b->raman && st.iir;
+  const bool all_dense = st.all_dense, any_dense = st.any_dense;
   // contraction tile: the largest power of two <= 256 whose U + pair-field tile fits in
   // 100 KB (the pair fields are formed in the tile with Raman on and off)
   const int rows = std::max(Mmax + Pall, 1);
@@ -1540,23 +1571,67 @@ bool batch_shape(mmp_batch* b) {
   }
   const int stage_terms = sr ? 0 : (pchunk ? 1 : (dense != 1 && !tc && smem + max_terms * staged <= 200 * 1024 ? 1 : 0));
   if (stage_terms && !pchunk) smem += max_terms * staged;
-  const bool changed = Mmax != b->Mmax || Pmax != b->Pmax || TT != b->TT || smem != b->contract_smem ||
-                       stage_terms != b->stage_terms || span != b->span || iir != b->raman_iir ||
-                       fused != b->raman_fused || dense != b->dense || tc != b->tc || pchunk != b->pchunk ||
-                       sr != b->sr;
-  b->dense = dense;
-  b->tc = tc;
-  b->pchunk = pchunk;
-  b->sr = sr;
-  b->raman_iir = iir;
-  b->raman_fused = fused;
-  b->kernels_per_step = b->tab.s * ((b->raman ? (fused ? 2 : 1) : 0) + 2);
-  b->span = span;
-  b->Mmax = Mmax;
-  b->Pmax = Pmax;
-  b->TT = TT;
-  b->contract_smem = smem;
-  b->stage_terms = stage_terms;
+  Shape sh;
+  sh.Mmax = Mmax;
+  sh.Pmax = Pmax;
+  sh.TT = TT;
+  sh.dense = dense;
+  sh.pchunk = pchunk;
+  sh.stage_terms = stage_terms;
+  sh.tc = tc;
+  sh.sr = sr;
+  sh.fused = fused;
+  sh.iir = iir;
+  sh.smem = smem;
+  sh.span = span;
+  return sh;
+}
+
+// Would the solve `p` run in batch `b` (a served pool) on exactly the kernels and tiles it
+// runs alone? True when a batch of it alone, `b` with it added and `b` as it is all have
+// the same shape (an empty `b`: the first two). The shape depends on maxima over the
+// solves (the tile shrinks as rows grow, tall tiles take the serial-recurrence form, dense Q
+// the dense form), so a solve joins only pools whose maxima lead to its own choices, and
+// since every solve in a pool then has the pool's shape alone, one leaving does not change
+// it either.
+bool joins_same_kernels(const mmp_batch* b, const mmp_params* p) {
+  Member m;
+  host_setup(p, m);
+  bool iir = false;
+  if (b->raman && p->raman_response) {
+    std::complex<double> lam, c;
+    iir = fit_damped_sinusoid(p->raman_response, p->nt, lam, c);
+  }
+  const bool dense_ok = dense_wanted(b, m);
+  ShapeStats alone;
+  add_stats(alone, b, m, iir, dense_ok, 1);
+  ShapeStats with = batch_stats(b);
+  const bool empty = with.span == 0;
+  add_stats(with, b, m, iir, dense_ok, 1);
+  const Shape w = choose_shape(b, with);
+  if (!same_kernels(choose_shape(b, alone), w)) return false;
+  return empty || same_kernels(choose_shape(b, batch_stats(b)), w);
+}
+
+bool batch_shape(mmp_batch* b) {
+  const Shape sh = choose_shape(b, batch_stats(b));
+  const bool changed = sh.Mmax != b->Mmax || sh.Pmax != b->Pmax || sh.TT != b->TT || sh.smem != b->contract_smem ||
+                       sh.stage_terms != b->stage_terms || sh.span != b->span || sh.iir != b->raman_iir ||
+                       sh.fused != b->raman_fused || sh.dense != b->dense || sh.tc != b->tc ||
+                       sh.pchunk != b->pchunk || sh.sr != b->sr;
+  b->dense = sh.dense;
+  b->tc = sh.tc;
+  b->pchunk = sh.pchunk;
+  b->sr = sh.sr;
+  b->raman_iir = sh.iir;
+  b->raman_fused = sh.fused;
+  b->kernels_per_step = b->tab.s * ((b->raman ? (sh.fused ? 2 : 1) : 0) + 2);
+  b->span = sh.span;
+  b->Mmax = sh.Mmax;
+  b->Pmax = sh.Pmax;
+  b->TT = sh.TT;
+  b->contract_smem = sh.smem;
+  b->stage_terms = sh.stage_terms;
   if (changed && b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;

@@ -4,7 +4,9 @@ step count falls on the loop's replay boundaries; the memory budget is honoured 
 a failing solve fails alone.
 
 Results are compared bit for bit: a served solve runs the same kernels on the same
-data as a standalone one (the pool only adds other solves to the launch grids)."""
+data as a standalone one (a request joins only a pool whose launch shape, which depends
+on its largest solves, is the one it has alone; the pool only adds other solves to the
+launch grids)."""
 import time
 
 import numpy as np
@@ -77,6 +79,27 @@ def test_dense_requests_on_the_tensor_cores_in_a_pool(mmp):
             alone, sinfo = s.result(), s.info()
         assert sinfo["tensor_core_contraction"] == 1
         assert np.array_equal(out, alone)
+
+
+def test_requests_of_different_kernel_shapes_keep_their_own(mmp):
+    # With about 200 pair fields per request the contraction runs on the serial-recurrence
+    # form (k_contract_sr); a pool chooses its form and tiles from its largest request, so
+    # a request that is not tall alone (M + P <= 200: M=20, 177 pair fields) must not be
+    # served in a pool of tall ones. Each request here gets the bits of its standalone
+    # solve; the tall ones also finish at different steps while their pool runs.
+    cases = [(310, 22, 1200, 5, True), (311, 20, 1400, 3, False), (312, 22, 1200, 8, True), (313, 21, 1600, 4, True)]
+    probs = [W.small_case(seed=seed, M=m, nt=256, n_steps=n, raman=True, nnz_target=nnz, physical_order=True,
+                          peak_w=20.0) for seed, m, nnz, n, _ in cases]
+    with mmp.Server(max_slots=4, steps_per_tick=2) as sv:
+        ids = [sv.submit(p) for p in probs]
+        outs = [sv.wait(i, timeout=120) for i in ids]
+    for (seed, _, _, _, tall), p, (out, info) in zip(cases, probs, outs):
+        assert info["status"] == 0 and info["steps"] == p.n_steps, seed
+        with mmp.Solver(p) as s:
+            s.propagate(p.n_steps)
+            alone, sinfo = s.result(), s.info()
+        assert (sinfo["contract_sub_block"] > 0) == tall, seed
+        assert np.array_equal(out, alone), seed
 
 
 def test_memory_budget_serialises_and_rejects(mmp):
