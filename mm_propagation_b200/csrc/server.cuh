@@ -40,6 +40,11 @@ struct Request {
   uint64_t steps = 0;
   double t_submit = 0, t_start = -1, t_done = -1;
   std::vector<double> result;
+  // its device bytes and its contribution to a pool's launch shape, computed once
+  // (worker thread only)
+  bool sized = false, counted = false;
+  size_t need = 0;
+  SolveCounts counts;
   // placement while running (worker thread only)
   int pool = -1;
   uint32_t slot = 0;
@@ -236,8 +241,12 @@ bool admit_waiting(mmp_server* sv) {
         Pool& pl = sv->pools[i];
         // a request joins only a pool where it runs the kernels and tiles it runs alone,
         // so its fields are those of a standalone solve whatever it shares the pool with
-        if (pl.used >= (int)pl.b->capacity || !same_shape(pl.b, &r->p) || !joins_same_kernels(pl.b, &r->p))
-          continue;
+        if (pl.used >= (int)pl.b->capacity || !same_shape(pl.b, &r->p)) continue;
+        if (!r->counted) {
+          r->counts = solve_counts(&r->p);
+          r->counted = true;
+        }
+        if (!joins_same_kernels(pl.b, r->counts)) continue;
         if (pl.in_flight) {
           deferred = true;  // a pool with room is busy: try again after its replay
           continue;
@@ -246,7 +255,11 @@ bool admit_waiting(mmp_server* sv) {
         break;
       }
       if (pi < 0 && deferred) continue;
-      const size_t need = footprint(&r->p);
+      if (!r->sized) {  // host setup once per request, not on every pass over the queue
+        r->need = footprint(&r->p);
+        r->sized = true;
+      }
+      const size_t need = r->need;
       if (sv->used_bytes + need > sv->cfg.memory_budget) {
         if (sv->used_bytes != 0) continue;  // first fit: try the next waiting request
         rc = fail(MMP_ENOMEM, "request larger than the server's memory budget");

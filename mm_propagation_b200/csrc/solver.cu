@@ -1431,26 +1431,41 @@ struct ShapeStats {
   uint32_t span = 0;
 };
 
-void add_stats(ShapeStats& st, const mmp_batch* b, const Member& s, bool iir, bool dense_ok, uint32_t span) {
-  st.iir = st.iir && iir;
-  st.all_dense = st.all_dense && dense_ok;
-  st.any_dense = st.any_dense || dense_ok;
+// One solve's part in them: what its host setup gives (see solve_counts).
+struct SolveCounts {
+  int M = 0;
+  size_t pairs = 0, terms = 0, sr_terms = 0;
+  bool iir = false, dense_ok = false;
+};
+
+void add_stats(ShapeStats& st, const mmp_batch* b, const SolveCounts& c, uint32_t span) {
+  st.iir = st.iir && c.iir;
+  st.all_dense = st.all_dense && c.dense_ok;
+  st.any_dense = st.any_dense || c.dense_ok;
   st.span = std::max(st.span, span);
-  st.Mmax = std::max(st.Mmax, (int)s.M);
-  st.Mmin = std::min(st.Mmin, (int)s.M);
-  st.Pmax = std::max(st.Pmax, (int)(b->raman ? s.pairs.size() : 0));
-  st.Pall = std::max(st.Pall, (int)s.pairs.size());
-  st.max_terms = std::max(st.max_terms, s.terms.size());
-  st.max_sr_terms = std::max(st.max_sr_terms, s.sr_kq.size());
+  st.Mmax = std::max(st.Mmax, c.M);
+  st.Mmin = std::min(st.Mmin, c.M);
+  st.Pmax = std::max(st.Pmax, (int)(b->raman ? c.pairs : 0));
+  st.Pall = std::max(st.Pall, (int)c.pairs);
+  st.max_terms = std::max(st.max_terms, c.terms);
+  st.max_sr_terms = std::max(st.max_sr_terms, c.sr_terms);
+}
+
+SolveCounts member_counts(const Member& s) {
+  SolveCounts c;
+  c.M = (int)s.M;
+  c.pairs = s.pairs.size();
+  c.terms = s.terms.size();
+  c.sr_terms = s.sr_kq.size();
+  c.iir = s.desc.iir != 0;
+  c.dense_ok = s.dense_ok;
+  return c;
 }
 
 ShapeStats batch_stats(const mmp_batch* b) {
   ShapeStats st;
   for (size_t i = 0; i < b->members.size(); ++i)
-    if (b->active[i]) {
-      const Member& s = b->members[i];
-      add_stats(st, b, s, s.desc.iir != 0, s.dense_ok, (uint32_t)i + 1);
-    }
+    if (b->active[i]) add_stats(st, b, member_counts(b->members[i]), (uint32_t)i + 1);
   return st;
 }
 
@@ -1587,27 +1602,33 @@ Shape choose_shape(const mmp_batch* b, const ShapeStats& st) {
   return sh;
 }
 
-// Would the solve `p` run in batch `b` (a served pool) on exactly the kernels and tiles it
+// Would the solve with counts `c` run in batch `b` (a served pool) on exactly the kernels and tiles it
 // runs alone? True when a batch of it alone, `b` with it added and `b` as it is all have
 // the same shape (an empty `b`: the first two). The shape depends on maxima over the
 // solves (the tile shrinks as rows grow, tall tiles take the serial-recurrence form, dense Q
 // the dense form), so a solve joins only pools whose maxima lead to its own choices, and
 // since every solve in a pool then has the pool's shape alone, one leaving does not change
 // it either.
-bool joins_same_kernels(const mmp_batch* b, const mmp_params* p) {
+// A solve's counts from its parameters alone (the host setup a member gets at creation).
+SolveCounts solve_counts(const mmp_params* p) {
   Member m;
   host_setup(p, m);
-  bool iir = false;
-  if (b->raman && p->raman_response) {
-    std::complex<double> lam, c;
-    iir = fit_damped_sinusoid(p->raman_response, p->nt, lam, c);
+  SolveCounts c = member_counts(m);
+  c.iir = false;
+  if (p->raman && p->raman_response) {
+    std::complex<double> lam, cc;
+    c.iir = fit_damped_sinusoid(p->raman_response, p->nt, lam, cc);
   }
-  const bool dense_ok = dense_wanted(b, m);
+  c.dense_ok = dense_wanted(nullptr, m);
+  return c;
+}
+
+bool joins_same_kernels(const mmp_batch* b, const SolveCounts& c) {
   ShapeStats alone;
-  add_stats(alone, b, m, iir, dense_ok, 1);
+  add_stats(alone, b, c, 1);
   ShapeStats with = batch_stats(b);
   const bool empty = with.span == 0;
-  add_stats(with, b, m, iir, dense_ok, 1);
+  add_stats(with, b, c, 1);
   const Shape w = choose_shape(b, with);
   if (!same_kernels(choose_shape(b, alone), w)) return false;
   return empty || same_kernels(choose_shape(b, batch_stats(b)), w);

@@ -182,7 +182,7 @@ template <typename G> __device__ __forceinline__ int cluster_rank() {
 
 // Common start of a row kernel: shared memory (the row, then the twiddle table).
 #define MMP_ROW_SMEM()                                                 \
-  extern __shared__ __align__(16) unsigned char smem_raw[];            \
+  extern __shared__ __align__(128) unsigned char smem_raw[];            \
   V* s = reinterpret_cast<V*>(smem_raw);
 
 // ---- k_prime: U for stage `stage` from psi_hat (and the stored N_hat_j) -------------------
@@ -374,7 +374,7 @@ template <typename T>
 __global__ void __launch_bounds__(512) k_raman_scan(const SolveDesc* __restrict__ descs, int nt, int seg) {
   using V = c2<T>;
   constexpr int kMaxSeg = 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   V* sv = reinterpret_cast<V*>(smem_raw);  // padded: element i at pad(i)
   __shared__ Affine warp_tot[17];
   __shared__ Affine seg_map[kMaxSeg];
@@ -1113,7 +1113,7 @@ __device__ __forceinline__ void tile_pair_recurrence(const TileScan<T>& ts, cons
 template <typename T>
 __global__ void __launch_bounds__(256) k_raman_agg(const SolveDesc* __restrict__ descs, int nt, int TT) {
   using V = c2<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const SolveDesc& d = descs[blockIdx.y];
   const int tile = blockIdx.x, t0 = tile * TT;
   if (t0 >= nt || d.M == 0) return;  // empty slot
@@ -1662,7 +1662,7 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 3 : 1))
   constexpr int J = kSrSub / 2;  // sample pairs per sub-block
   constexpr int RS = J + 1;      // row stride in sample pairs: consecutive rows start 16 bytes apart
                                  // mod 128, so a quarter warp's rows fall on different banks
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TB;
   if (t0 >= nt || d.M == 0) return;               // empty slot
@@ -1842,7 +1842,7 @@ __global__ void __launch_bounds__(kSrThreads, (sizeof(T) == 4 ? 4 : 2))
   using SP = SrPair<T>;
   constexpr int J = kSrSub / 2;
   constexpr int RS = J + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const SolveDesc& d = descs[blockIdx.y];
   const int t0 = blockIdx.x * TB;
   if (t0 >= nt || d.M == 0) return;            // empty slot
