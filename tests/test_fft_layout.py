@@ -176,3 +176,35 @@ def test_transform_matches_numpy(fp64, logn, xc):
         for w in range(gm.NL):
             y[gm.time_of_w(r, w)] = S[r][gm.sidx(gm.local_of_w(w))]
     assert np.abs(y / gm.N - x).max() <= 1e-12 * np.abs(x).max()
+
+
+@pytest.mark.parametrize("fp64,logn,xc", GEOMETRIES)
+def test_pass_offsets_by_constant_stride(fp64, logn, xc):
+    # stockham_pass computes one padded offset per butterfly and steps by a constant where
+    # the elements lie a multiple of 32 apart (reads: stride NB/R when it is one; writes:
+    # Ns = 2^logns from 32 up, and R consecutive elements at logns = 0)
+    gm = Geo(fp64, logn, xc)
+    passes = [gm.LOGE] * (gm.LOGNLG // gm.LOGE) + ([gm.LOGNLG % gm.LOGE] if gm.LOGNLG % gm.LOGE else [])
+    sidx = np.vectorize(gm.sidx)
+    tid = np.arange(gm.NTHR)
+    logns = 0
+    for logr in passes:
+        r, logj = 1 << logr, gm.LOGNLG - logr
+        stride = gm.NLG // r
+        for bf in range(gm.E // r):
+            ja = tid + bf * gm.NTHR
+            base, j = (ja >> logj) << gm.LOGNLG, ja & ((1 << logj) - 1)
+            if stride % 32 == 0:
+                a0 = sidx(base + j)
+                for q in range(r):
+                    assert (a0 + q * (stride + stride // 32) == sidx(base + j + q * stride)).all()
+            jm = j & ((1 << logns) - 1)
+            idx = ((j >> logns) << (logns + logr)) + jm
+            w0 = sidx(base + idx)
+            for q in range(r):
+                ref = sidx(base + idx + (q << logns))
+                if logns >= 5:
+                    assert (w0 + q * ((1 << logns) + (1 << (logns - 5))) == ref).all()
+                elif logns == 0:
+                    assert (w0 + q == ref).all()
+        logns += logr
