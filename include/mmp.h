@@ -237,14 +237,15 @@ void mmp_batch_destroy(mmp_batch* b);
 
 /* ---- serving: a request loop with continuous batching ---------------------------------
  * No counterpart in the reference (one solve per process). A worker thread owns the
- * device. Requests are grouped by kernel shape (nt, precision, Raman, RK tableau) into
+ * device. Requests are grouped by kernel shape (nt, precision, Raman, RK tableau, and the
+ * contraction form and tile each would get alone) into
  * slot pools; each pool advances all its solves with one captured multi-step CUDA
  * graph per replay on its own stream, so different pools overlap on the device.
  * Between replays the worker retires finished solves (their result is copied to host
  * memory) and admits waiting ones into free slots, first fit, as long as the device
  * memory they need stays within the budget. Each solve stops at its own n_steps on
- * the device. Results equal those of mmp_solver_create + mmp_propagate(n_steps) +
- * mmp_get_result for the same parameters. */
+ * the device. Results equal, bit for bit, those of mmp_solver_create +
+ * mmp_propagate(n_steps) + mmp_get_result for the same parameters. */
 typedef struct mmp_server mmp_server;
 typedef struct mmp_server_config {
   uint64_t memory_budget;   /* device bytes for solve state; 0 = 80% of free memory */
