@@ -31,6 +31,8 @@ struct mmp_shim_plan_s {
   cplx* tw;        /* concatenated per-pass tables: w1, w2, w3 for radix 4; w1 for radix 2 */
   size_t tw_off[40];
   cplx* dft_tw;    /* direct-DFT table for non-power-of-two sizes, length n */
+  fftw_complex* in;   /* the arrays the plan was made for (fftw_execute) */
+  fftw_complex* out;
 };
 
 static const double kTwoPi = 6.283185307179586476925286766559;
@@ -56,10 +58,12 @@ static cplx unit_root(double num, double den, int sign) {
 }
 
 fftw_plan fftw_plan_dft_1d(int n, fftw_complex* in, fftw_complex* out, int sign, unsigned flags) {
-  (void)in; (void)out; (void)flags;
+  (void)flags;
   if (n <= 0) return NULL;
   struct mmp_shim_plan_s* p = (struct mmp_shim_plan_s*)calloc(1, sizeof(*p));
   p->n = n;
+  p->in = in;
+  p->out = out;
   p->sign = (sign < 0) ? -1 : 1;
   p->pow2 = (n & (n - 1)) == 0;
   if (p->pow2) {
@@ -223,4 +227,7 @@ void fftw_execute_dft(const fftw_plan p, fftw_complex* in, fftw_complex* out) {
     exec_direct(p, (const cplx*)in, (cplx*)out);
 }
 
-void fftw_execute(const fftw_plan p) { (void)p; /* plans here carry no bound arrays */ }
+/* FFTW's fftw_execute: the plan on the arrays it was made for */
+void fftw_execute(const fftw_plan p) {
+  if (p) fftw_execute_dft(p, p->in, p->out);
+}

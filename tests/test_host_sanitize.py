@@ -1,5 +1,5 @@
-"""The C ABI's host code under AddressSanitizer and UndefinedBehaviorSanitizer (no device
-needed). The library's host units (solver.cu, noalloc.cu, io.cpp) are rebuilt with both
+"""The C ABI's host code, and the oracle's FFT shim, under AddressSanitizer and
+UndefinedBehaviorSanitizer (no device needed). The library's host units (solver.cu, noalloc.cu, io.cpp) are rebuilt with both
 sanitizers, linked to the already-built kernel objects, and driven through their
 host-only paths by tests/sanitize/host_capi.cpp: parameter validation with valid and
 malformed inputs, RK tableaus, dense-coupling conversion, the MAT-file and text writers
@@ -59,3 +59,18 @@ def test_host_paths_are_clean_under_asan_and_ubsan(tmp_path):
     assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-4000:]
     assert "all checks passed" in r.stdout
     assert (tmp_path / "out.mat").stat().st_size > 0 and (tmp_path / "abs.txt").stat().st_size > 0
+
+
+def test_oracle_fft_shim_is_clean_under_asan_and_ubsan(tmp_path):
+    # the FFTW-API shim the oracle links the reference's CPU sources against (our code;
+    # the reference's own sources are not run under the sanitizers: they carry a known
+    # delete / new[] mismatch, src/ComplexArray.cpp:32)
+    shim = os.path.join(ROOT, "oracle", "fftw_shim")
+    exe = str(tmp_path / "shim_fft")
+    _run(["gcc", "-std=c11", "-O1", "-g", "-D_DEFAULT_SOURCE", "-I", shim, os.path.join(shim, "fftw3_shim.c"),
+          os.path.join(HERE, "sanitize", "shim_fft.c"), "-o", exe, "-lm"] + SAN)
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:exitcode=23",
+               UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1:exitcode=24")
+    r = subprocess.run([exe], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-4000:]
+    assert "all checks passed" in r.stdout
