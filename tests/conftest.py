@@ -24,7 +24,7 @@ def has_gpu() -> bool:
 
 @pytest.fixture(scope="session")
 def mmp():
-    """The product library; on a GPU box its absence is an error, not a skip."""
+    """The product library; on a machine with a GPU its absence is an error, not a skip."""
     import mm_propagation_b200 as m
     m.lib()
     return m
