@@ -132,7 +132,8 @@ typedef struct mmp_solver mmp_solver;
 /* Validate parameters without touching the device. Checks the conditions the
  * MATLAB front-end checks (matlab/mm_propagation.cpp:341-527) plus the ones
  * under which the reference silently produces NaN/Inf (max|beta2| == 0,
- * max|Q| == 0, T0 <= 0, fewer than 3 dispersion orders, indices >= M).
+ * max|Q| == 0, nonlinearity_const == 0, T0 <= 0, fewer than 3 dispersion orders,
+ * indices >= M).
  * On failure writes a one-line reason into msg (if msg != NULL). */
 int mmp_validate_params(const mmp_params* params, char* msg, size_t msg_len);
 

@@ -445,6 +445,12 @@ int validate(const mmp_params* p, std::string& why) {
   if (!(p->fiber_length > 0) || !std::isfinite(p->fiber_length)) { why = "fiber_length must be > 0"; return MMP_EINVAL; }
   if (p->n_steps == 0) { why = "n_steps must be >= 1"; return MMP_EINVAL; }
   if (!std::isfinite(p->nonlinearity_const)) { why = "nonlinearity_const must be finite"; return MMP_EINVAL; }
+  if (p->nonlinearity_const == 0) {
+    // the reference then scales the fields by 0 and its getResult divides by 0: all NaN
+    // (src/MultimodePropagation.cpp:53, :61; src/MultimodePropagation_CPU.cpp:100)
+    why = "nonlinearity_const is 0: the conversion factor sqrt(|gamma| LD) sqrt(max|Q|) is 0";
+    return MMP_EINVAL;
+  }
   double mb2 = 0, mq = 0;
   for (uint32_t m = 0; m < p->n_modes; ++m) {
     for (uint32_t i = 0; i < p->n_beta; ++i)

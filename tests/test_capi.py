@@ -57,6 +57,8 @@ def test_validate_accepts_workloads():
     (lambda p: p.replace(nt=100, initial_fields=p.initial_fields[:, :100],
                          raman_response=p.raman_response[:100]), capi.MMP_ENOTSUP),
     (lambda p: p.replace(raman_response=None), capi.MMP_EINVAL),
+    # the reference's conversion factor sqrt(|gamma| LD max|Q|) is then 0 and its result 0/0
+    (lambda p: p.replace(nonlinearity_const=0.0), capi.MMP_EINVAL),
 ])
 def test_validate_rejects(mutate, code):
     base = W.grin2(nt=256, n_steps=10)
